@@ -1,0 +1,165 @@
+/*
+ * meanas_fdfd.h -- C ABI of the B200 FDFD solve path (libmeanas_fdfd.so).
+ *
+ * Drop-in for the hot path behind meanas.fdfd.solvers.generic()
+ * (reference: meanas/fdfd/solvers.py:66-141): the E-field wave operator
+ *     A0 = pe (ch pm mu^-1 ce - omega^2 eps) pe          (meanas/fdfd/operators.py:40-96)
+ * applied matrix-free on the Yee grid, its symmetrised form Pl A0 Pr
+ * (meanas/fdfd/operators.py:99-123), and the Krylov solve of A0 E = -i omega J.
+ *
+ * Conventions
+ *   - Fields are 3 x X x Y x Z, C order (z fastest), as meanas.fdmath.vec() makes
+ *     them (meanas/fdmath/vectorization.py:51-68); N = X*Y*Z cells, 3N elements.
+ *   - Complex arrays are interleaved (re, im): complex128 = 2 doubles,
+ *     complex64 = 2 floats.
+ *   - Every pointer to a field or table is DEVICE memory of the current CUDA
+ *     device; `stream` is a cudaStream_t (NULL = legacy default stream).
+ *   - No function allocates device memory: callers size and pass workspaces.
+ *   - Return codes: 0 = success; > 0 = the solver stopped without meeting its
+ *     tolerance (an FDFD_STATUS_* value); < 0 = argument or CUDA error, with the
+ *     message available from fdfd_last_error() (per calling thread).
+ */
+#ifndef MEANAS_FDFD_H
+#define MEANAS_FDFD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FDFD_ABI_VERSION 1
+
+/* solver status (fdfd_solve_info.status and positive return codes) */
+#define FDFD_STATUS_CONVERGED 1
+#define FDFD_STATUS_MAXITER 2
+#define FDFD_STATUS_BREAKDOWN 3
+#define FDFD_STATUS_NONFINITE 4
+
+/* error codes (negative returns) */
+#define FDFD_ERR_ARG (-1)
+#define FDFD_ERR_CUDA (-2)
+#define FDFD_ERR_WORKSPACE (-3)
+
+/* fdfd_grid_desc.flags */
+#define FDFD_GRID_FP32 1 /* also build complex64 tables (needed by FDFD_METHOD_MIXED) */
+
+/* operators for fdfd_apply */
+#define FDFD_OP_A0 0      /* y = A0 x                                        */
+#define FDFD_OP_SYM 1     /* y = Pl A0 Pr x  (the matrix generic() hands QMR) */
+#define FDFD_OP_SYM_H 2   /* y = (Pl A0 Pr)^H x  (generic(adjoint=True))     */
+
+/* precisions */
+#define FDFD_C128 0
+#define FDFD_C64 1
+
+/* solver methods */
+#define FDFD_METHOD_COCG 0     /* complex128 COCG on the symmetrised system            */
+#define FDFD_METHOD_MIXED 1    /* complex64 BiCGSTAB inner + complex128 refinement     */
+#define FDFD_METHOD_BICGSTAB 2 /* complex128 BiCGSTAB                                  */
+
+/* stopping criteria */
+#define FDFD_CRIT_TRUE 0    /* ||b0 - A0 E|| <= max(rtol ||b0||, atol), b0 = -i omega J      */
+#define FDFD_CRIT_PRECOND 1 /* scipy's test on the symmetrised system generic() builds:
+                               ||Pl (b0 - A0 E)|| <= max(rtol ||Pl b0||, atol)            */
+
+typedef struct fdfd_plan fdfd_plan;
+
+/* Grid, material and frequency: the arguments of generic() that define A0. */
+typedef struct fdfd_grid_desc {
+  int32_t shape[3];     /* X, Y, Z (each >= 1)                                     */
+  int32_t flags;        /* FDFD_GRID_*                                             */
+  double omega[2];      /* complex angular frequency (re, im)                      */
+  const void* dxe[3];   /* complex128[shape[a]]: dxes[0][a] (E-grid cell widths)   */
+  const void* dxh[3];   /* complex128[shape[a]]: dxes[1][a] (H-grid cell widths)   */
+  const void* inv_dxe[3]; /* optional complex128 1/dxe (NULL: computed on device)  */
+  const void* inv_dxh[3]; /* optional complex128 1/dxh                             */
+  const double* epsilon;  /* float64[3N]; referenced, not copied: keep it alive    */
+  const double* mu;       /* float64[3N] or NULL (mu = 1)                          */
+  const double* pec;      /* float64[3N] or NULL; nonzero = PEC on that E component */
+  const double* pmc;      /* float64[3N] or NULL; nonzero = PMC on that H component */
+} fdfd_grid_desc;
+
+typedef struct fdfd_solve_opts {
+  int32_t method;        /* FDFD_METHOD_*                                           */
+  int32_t criterion;     /* FDFD_CRIT_*                                             */
+  int32_t adjoint;       /* nonzero: solve A0^H E = -i omega J (generic(adjoint=True)) */
+  int32_t maxiter;       /* Krylov iteration cap (inner iterations summed for MIXED) */
+  double rtol;
+  double atol;
+  int32_t has_guess;     /* nonzero: E holds an initial guess on entry (E_guess)    */
+  int32_t chunk;         /* iterations per launch batch / CUDA graph (0 = default)  */
+  int32_t use_graph;     /* nonzero: replay iteration batches as CUDA graphs        */
+  int32_t max_outer;     /* MIXED: refinement steps cap (0 = default)               */
+  double inner_rtol;     /* MIXED: residual reduction per inner solve (0 = default) */
+  double* history;       /* optional device float64[maxiter + 1]: relative residuals */
+  int32_t profile;       /* nonzero: time every iteration kernel with CUDA events (no
+                            graphs); fills the *_ms / *_launches fields of the info  */
+  int32_t pad_;
+} fdfd_solve_opts;
+
+typedef struct fdfd_solve_info {
+  int32_t status;          /* FDFD_STATUS_*                                          */
+  int32_t iterations;      /* Krylov iterations (inner iterations summed for MIXED)  */
+  int32_t outer_iterations;/* MIXED refinement steps                                 */
+  int32_t kernel_launches; /* kernels launched by this call                          */
+  double residual;         /* ||b0 - A0 E|| / ||b0||, FP64, recomputed at the end    */
+  double residual_pc;      /* ||Pl (b0 - A0 E)|| / ||Pl b0||                         */
+  /* with opts->profile: device time of the iteration kernels, by kind
+     [0] COCG stencil pass  [1] COCG pointwise pass
+     [2] BiCGSTAB P pass    [3] BiCGSTAB S pass        (ms summed, launch counts) */
+  double kernel_ms[4];
+  int32_t kernel_count[4];
+} fdfd_solve_info;
+
+/* Version of this ABI (FDFD_ABI_VERSION). */
+int fdfd_abi_version(void);
+
+/* Message of the last error on the calling thread ("" if none). */
+const char* fdfd_last_error(void);
+
+/* Device bytes the plan keeps (1/mu, packed PEC/PMC bits, 1D tables, complex64
+ * copies when FDFD_GRID_FP32 is set).  Replaces the sparse assembly of
+ * meanas/fdfd/operators.py:76-96 (no matrix is ever stored). */
+int fdfd_plan_workspace_bytes(const fdfd_grid_desc* desc, size_t* bytes);
+
+/* Build a plan in caller-provided device memory `ws` (>= fdfd_plan_workspace_bytes,
+ * 256-byte aligned).  Enqueues its set-up kernels on `stream`. */
+int fdfd_plan_create(const fdfd_grid_desc* desc, void* ws, size_t ws_bytes, void* stream,
+                     fdfd_plan** out);
+
+/* Release the host-side plan object (the caller owns `ws`). */
+int fdfd_plan_destroy(fdfd_plan* plan);
+
+/* Override the x-planes-per-CTA tiling for one precision (autotuner hook). */
+int fdfd_plan_set_xchunk(fdfd_plan* plan, int32_t precision, int32_t xchunk);
+
+/* Matrix-free operator product y = op(x) in complex128 or complex64 (x, y: 3N).
+ * FDFD_OP_A0 replaces operators.e_full(...) @ x (meanas/fdfd/operators.py:40-96);
+ * FDFD_OP_SYM replaces (Pl @ A0 @ Pr) @ x (meanas/fdfd/solvers.py:116-125);
+ * FDFD_OP_SYM_H replaces (Pl @ A0 @ Pr).H @ x (meanas/fdfd/solvers.py:119-122). */
+int fdfd_apply(fdfd_plan* plan, int32_t op, int32_t precision, const void* x, void* y, void* stream);
+
+/* Device workspace bytes fdfd_solve needs for these options. */
+int fdfd_solve_workspace_bytes(const fdfd_plan* plan, const fdfd_solve_opts* opts, size_t* bytes);
+
+/* Solve A0 E = -i omega J (or the adjoint) for E (complex128, 3N).
+ * Replaces meanas/fdfd/solvers.py:66-141 (generic) with its default
+ * matrix_solver _scipy_qmr (:21-63).  J: complex128[3N].  E: complex128[3N]
+ * output (and initial guess when opts->has_guess).  Synchronous with respect to
+ * the host (it polls the device for convergence); all work runs on `stream`. */
+int fdfd_solve(fdfd_plan* plan, const fdfd_solve_opts* opts, const void* J, void* E, void* ws,
+               size_t ws_bytes, fdfd_solve_info* info, void* stream);
+
+/* FP64 residual norms of a field: out[0] = ||b0 - A0 E||, out[1] = ||Pl (b0 - A0 E)||,
+ * out[2] = ||b0||, out[3] = ||Pl b0|| with b0 = -i omega J
+ * (the check of meanas/test/test_fdfd.py:14-18).  `ws` >= fdfd_residual_workspace_bytes. */
+int fdfd_residual_workspace_bytes(const fdfd_plan* plan, size_t* bytes);
+int fdfd_residual(fdfd_plan* plan, const void* E, const void* J, double out[4], void* ws,
+                  size_t ws_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MEANAS_FDFD_H */

@@ -1,0 +1,864 @@
+// Host side of libmeanas_fdfd.so: plans, solver drivers and the C ABI of
+// include/meanas_fdfd.h.  All device memory comes from the caller (workspaces);
+// the only allocations here are a host plan object, a private capture stream,
+// two events and a few bytes of pinned host memory for convergence polling.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/meanas_fdfd.h"
+#include "fdfd_ops.cuh"
+
+using namespace fdfd;
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_err;
+
+static int set_err(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CK(call)                                                                           \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess) return set_err(FDFD_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+#define CKL()                                                                              \
+  do {                                                                                     \
+    cudaError_t e_ = cudaGetLastError();                                                   \
+    if (e_ != cudaSuccess) return set_err(FDFD_ERR_CUDA, "kernel launch: %s", cudaGetErrorString(e_)); \
+  } while (0)
+
+// ------------------------------------------------------------------ set-up kernels
+__global__ void k_mask_bits(const double* pec, const double* pmc, uint8_t* mask, long long N) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N; c += (long long)gridDim.x * blockDim.x) {
+    uint8_t m = 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      if (pec && pec[a * N + c] != 0.0) m |= (uint8_t)(1u << a);
+      if (pmc && pmc[a * N + c] != 0.0) m |= (uint8_t)(8u << a);
+    }
+    mask[c] = m;
+  }
+}
+
+__global__ void k_recip_real(const double* src, double* dst64, float* dst32, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double v = 1.0 / src[i];
+    dst64[i] = v;
+    if (dst32) dst32[i] = (float)v;
+  }
+}
+
+__global__ void k_to_f32(const double* src, float* dst, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = (float)src[i];
+}
+
+// 1D tables: copies of dx, and 1/dx (given, or computed with a scaled complex division)
+__global__ void k_tables(const double2* dx, const double2* inv_given, double2* dx64, double2* inv64,
+                         float2* dx32, float2* inv32, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double2 d = dx[i];
+    double2 r;
+    if (inv_given) {
+      r = inv_given[i];
+    } else {
+      const dcx q = ddiv({1.0, 0.0}, {d.x, d.y});
+      r = make_double2(q.re, q.im);
+    }
+    dx64[i] = d;
+    inv64[i] = r;
+    if (dx32) {
+      dx32[i] = make_float2((float)d.x, (float)d.y);
+      inv32[i] = make_float2((float)r.x, (float)r.y);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ plan
+struct Tiling {
+  int XC, ntz, nty, nxc;
+  long long nblocks;
+};
+
+struct GraphEntry {
+  int kind;
+  const void* a;
+  const void* b;
+  int chunk;
+  cudaGraphExec_t exec;
+};
+
+struct fdfd_plan {
+  int X, Y, Z;
+  long long N;
+  int flags;
+  double om_re, om_im;
+  bool flat;
+  bool has32;
+  int nsm;
+  int xc_override[2];
+  Geo<double> g64;
+  Geo<float> g32;
+  cudaStream_t cap;        // private stream for graph capture
+  cudaEvent_t ev[2];
+  int* h_poll;             // pinned: 2 x 4 ints (crit, iter, maxiter, status)
+  KState* h_state;         // pinned
+  std::vector<GraphEntry> graphs;
+  int launches;            // kernel launches counter for the current call
+  // optional per-kernel timing (fdfd_solve_opts.profile)
+  bool profiling;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<int, int>>> ev_marks;  // kind, (start idx, stop idx)
+  int ev_used;
+};
+
+// Bracket one launch with timing events when profiling (kind indexes kernel_ms).
+struct ProfScope {
+  fdfd_plan* P;
+  int kind, i0;
+  cudaStream_t s;
+  ProfScope(fdfd_plan* P_, int kind_, cudaStream_t s_) : P(P_), kind(kind_), i0(-1), s(s_) {
+    if (!P->profiling) return;
+    if (P->ev_used + 2 > (int)P->ev_pool.size()) {
+      for (int k = 0; k < 256; ++k) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return;
+        P->ev_pool.push_back(e);
+      }
+    }
+    i0 = P->ev_used;
+    P->ev_used += 2;
+    cudaEventRecord(P->ev_pool[i0], s);
+  }
+  ~ProfScope() {
+    if (i0 < 0) return;
+    cudaEventRecord(P->ev_pool[i0 + 1], s);
+    P->ev_marks.push_back({kind, {i0, i0 + 1}});
+  }
+};
+
+// Sum the recorded intervals into info (called after a stream synchronize).
+static void prof_collect(fdfd_plan* P, double* ms, int* cnt) {
+  for (auto& m : P->ev_marks) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, P->ev_pool[m.second.first], P->ev_pool[m.second.second]) == cudaSuccess) {
+      ms[m.first] += t;
+      cnt[m.first] += 1;
+    }
+  }
+  P->ev_marks.clear();
+  P->ev_used = 0;
+}
+
+static constexpr int FLAT_TY = 256;
+static constexpr int TZ3 = 32, TY3 = 8;
+
+static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+static Tiling make_tiling(const fdfd_plan* P, int precision) {
+  Tiling t;
+  const int TZ = P->flat ? 1 : TZ3, TY = P->flat ? FLAT_TY : TY3;
+  t.ntz = (P->Z + TZ - 1) / TZ;
+  t.nty = (P->Y + TY - 1) / TY;
+  const long long tiles = (long long)t.ntz * t.nty;
+  int xc = P->xc_override[precision];
+  if (xc <= 0) {
+    // aim for about 8 CTAs per SM in total (two waves at 4 resident CTAs per SM)
+    const long long target = 8LL * P->nsm;
+    long long need = (P->X * tiles + target - 1) / target;
+    xc = (int)std::max(4LL, std::min(64LL, need));
+  }
+  xc = std::min(xc, P->X);
+  t.XC = xc;
+  t.nxc = (P->X + xc - 1) / xc;
+  t.nblocks = tiles * t.nxc;
+  return t;
+}
+
+template <typename R>
+static Geo<R> geo_with(const Geo<R>& g, const Tiling& t) {
+  Geo<R> r = g;
+  r.XC = t.XC;
+  r.ntz = t.ntz;
+  r.nty = t.nty;
+  r.nxc = t.nxc;
+  return r;
+}
+
+static long long max_blocks(const fdfd_plan* P) {
+  long long m = make_tiling(P, 0).nblocks;
+  m = std::max(m, make_tiling(P, 1).nblocks);
+  // worst case over all x-chunk choices (the autotuner may pick XC = 1..)
+  const int TZ = P->flat ? 1 : TZ3, TY = P->flat ? FLAT_TY : TY3;
+  const long long tiles = (long long)((P->Z + TZ - 1) / TZ) * ((P->Y + TY - 1) / TY);
+  return std::max(m, tiles * P->X);
+}
+
+// ------------------------------------------------------------------ launches
+template <typename K>
+static void ensure_smem(K kern, size_t bytes) {
+  // only needed above the 48 KB default; remembered per kernel
+  static std::vector<const void*> done;
+  if (bytes <= 48 * 1024) return;
+  const void* key = (const void*)kern;
+  if (std::find(done.begin(), done.end(), key) != done.end()) return;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  done.push_back(key);
+}
+
+template <typename R, class Op>
+static int launch_stencil(fdfd_plan* P, const Geo<R>& g0, int precision, const Op& op, RedBuf rb,
+                          cudaStream_t s) {
+  const Tiling t = make_tiling(P, precision);
+  const Geo<R> g = geo_with(g0, t);
+  if (P->flat) {
+    using Sh = StencilShape<R, 1, FLAT_TY, true>;
+    auto kern = k_stencil<R, 1, FLAT_TY, true, Op>;
+    ensure_smem(kern, Sh::smem_bytes());
+    kern<<<(unsigned)t.nblocks, dim3(1, FLAT_TY), Sh::smem_bytes(), s>>>(g, op, rb);
+  } else {
+    using Sh = StencilShape<R, TZ3, TY3, false>;
+    auto kern = k_stencil<R, TZ3, TY3, false, Op>;
+    ensure_smem(kern, Sh::smem_bytes());
+    kern<<<(unsigned)t.nblocks, dim3(TZ3, TY3), Sh::smem_bytes(), s>>>(g, op, rb);
+  }
+  P->launches++;
+  CKL();
+  return 0;
+}
+
+template <typename R, class Op>
+static int launch_point(fdfd_plan* P, const Geo<R>& g0, int precision, const Op& op, RedBuf rb,
+                        cudaStream_t s) {
+  const Tiling t = make_tiling(P, precision);
+  const Geo<R> g = geo_with(g0, t);
+  if (P->flat) {
+    k_point<R, 1, FLAT_TY, Op><<<(unsigned)t.nblocks, dim3(1, FLAT_TY), 0, s>>>(g, op, rb);
+  } else {
+    k_point<R, TZ3, TY3, Op><<<(unsigned)t.nblocks, dim3(TZ3, TY3), 0, s>>>(g, op, rb);
+  }
+  P->launches++;
+  CKL();
+  return 0;
+}
+
+#define TRY(x)                 \
+  do {                         \
+    int rc_ = (x);             \
+    if (rc_ != 0) return rc_;  \
+  } while (0)
+
+// ------------------------------------------------------------------ C ABI: plan
+extern "C" int fdfd_abi_version(void) { return FDFD_ABI_VERSION; }
+
+extern "C" const char* fdfd_last_error(void) { return g_err.c_str(); }
+
+struct PlanLayout {
+  size_t muinv64, muinv32, eps32, mask, tab64, tab32, total;
+};
+
+static int plan_layout(const fdfd_grid_desc* d, PlanLayout* L) {
+  if (!d) return set_err(FDFD_ERR_ARG, "desc is NULL");
+  for (int a = 0; a < 3; ++a)
+    if (d->shape[a] < 1) return set_err(FDFD_ERR_ARG, "shape[%d] = %d must be >= 1", a, d->shape[a]);
+  const long long N = (long long)d->shape[0] * d->shape[1] * d->shape[2];
+  const long long S = (long long)d->shape[0] + d->shape[1] + d->shape[2];
+  const bool f32 = (d->flags & FDFD_GRID_FP32) != 0;
+  size_t off = 0;
+  L->muinv64 = off;
+  if (d->mu) off += align256(3 * N * sizeof(double));
+  L->muinv32 = off;
+  if (d->mu && f32) off += align256(3 * N * sizeof(float));
+  L->eps32 = off;
+  if (f32) off += align256(3 * N * sizeof(float));
+  L->mask = off;
+  if (d->pec || d->pmc) off += align256((size_t)N);
+  L->tab64 = off;
+  off += align256(4 * S * sizeof(double2));
+  L->tab32 = off;
+  if (f32) off += align256(4 * S * sizeof(float2));
+  L->total = off;
+  return 0;
+}
+
+extern "C" int fdfd_plan_workspace_bytes(const fdfd_grid_desc* desc, size_t* bytes) {
+  PlanLayout L;
+  TRY(plan_layout(desc, &L));
+  if (!bytes) return set_err(FDFD_ERR_ARG, "bytes is NULL");
+  *bytes = L.total;
+  return 0;
+}
+
+extern "C" int fdfd_plan_create(const fdfd_grid_desc* d, void* ws, size_t ws_bytes, void* stream,
+                                fdfd_plan** out) {
+  PlanLayout L;
+  TRY(plan_layout(d, &L));
+  if (!out) return set_err(FDFD_ERR_ARG, "out is NULL");
+  if (!d->epsilon) return set_err(FDFD_ERR_ARG, "epsilon is NULL");
+  for (int a = 0; a < 3; ++a)
+    if (!d->dxe[a] || !d->dxh[a]) return set_err(FDFD_ERR_ARG, "dxe/dxh[%d] is NULL", a);
+  if (ws_bytes < L.total || (L.total > 0 && !ws))
+    return set_err(FDFD_ERR_WORKSPACE, "plan workspace too small: %zu < %zu", ws_bytes, L.total);
+  if (((uintptr_t)ws & 255) != 0) return set_err(FDFD_ERR_ARG, "plan workspace must be 256-byte aligned");
+  cudaStream_t s = (cudaStream_t)stream;
+  fdfd_plan* P = new fdfd_plan();
+  P->X = d->shape[0];
+  P->Y = d->shape[1];
+  P->Z = d->shape[2];
+  P->N = (long long)P->X * P->Y * P->Z;
+  P->flags = d->flags;
+  P->om_re = d->omega[0];
+  P->om_im = d->omega[1];
+  P->flat = (P->Z == 1);
+  P->has32 = (d->flags & FDFD_GRID_FP32) != 0;
+  P->xc_override[0] = P->xc_override[1] = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&P->nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (P->nsm <= 0) P->nsm = 148;
+  auto cleanup = [&](int rc) {
+    delete P;
+    return rc;
+  };
+  if (cudaStreamCreateWithFlags(&P->cap, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&P->ev[0], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&P->ev[1], cudaEventDisableTiming) != cudaSuccess ||
+      cudaMallocHost((void**)&P->h_poll, 8 * sizeof(int)) != cudaSuccess ||
+      cudaMallocHost((void**)&P->h_state, sizeof(KState)) != cudaSuccess)
+    return cleanup(set_err(FDFD_ERR_CUDA, "plan: stream/event/pinned allocation failed"));
+
+  char* base = (char*)ws;
+  const long long N = P->N;
+  const int sh[3] = {P->X, P->Y, P->Z};
+  // 1D tables: [dxe | dxh | idxe | idxh], each X+Y+Z long (axis-major)
+  double2* t64 = (double2*)(base + L.tab64);
+  float2* t32 = P->has32 ? (float2*)(base + L.tab32) : nullptr;
+  const long long S = (long long)P->X + P->Y + P->Z;
+  long long aoff = 0;
+  for (int a = 0; a < 3; ++a) {
+    double2* dxe64 = t64 + aoff;
+    double2* dxh64 = t64 + S + aoff;
+    double2* ie64 = t64 + 2 * S + aoff;
+    double2* ih64 = t64 + 3 * S + aoff;
+    float2* dxe32 = t32 ? t32 + aoff : nullptr;
+    float2* dxh32 = t32 ? t32 + S + aoff : nullptr;
+    float2* ie32 = t32 ? t32 + 2 * S + aoff : nullptr;
+    float2* ih32 = t32 ? t32 + 3 * S + aoff : nullptr;
+    k_tables<<<(sh[a] + 255) / 256, 256, 0, s>>>((const double2*)d->dxe[a], (const double2*)d->inv_dxe[a], dxe64,
+                                                 ie64, dxe32, ie32, sh[a]);
+    k_tables<<<(sh[a] + 255) / 256, 256, 0, s>>>((const double2*)d->dxh[a], (const double2*)d->inv_dxh[a], dxh64,
+                                                 ih64, dxh32, ih32, sh[a]);
+    P->g64.dxe[a] = (const cx<double>*)dxe64;
+    P->g64.dxh[a] = (const cx<double>*)dxh64;
+    P->g64.idxe[a] = (const cx<double>*)ie64;
+    P->g64.idxh[a] = (const cx<double>*)ih64;
+    P->g32.dxe[a] = (const cx<float>*)dxe32;
+    P->g32.dxh[a] = (const cx<float>*)dxh32;
+    P->g32.idxe[a] = (const cx<float>*)ie32;
+    P->g32.idxh[a] = (const cx<float>*)ih32;
+    aoff += sh[a];
+  }
+  const int nb = (int)std::min<long long>((3 * N + 255) / 256, 148LL * 16);
+  P->g64.eps = d->epsilon;
+  P->g64.muinv = nullptr;
+  P->g32.muinv = nullptr;
+  P->g32.eps = nullptr;
+  if (d->mu) {
+    double* mi64 = (double*)(base + L.muinv64);
+    float* mi32 = P->has32 ? (float*)(base + L.muinv32) : nullptr;
+    k_recip_real<<<nb, 256, 0, s>>>(d->mu, mi64, mi32, 3 * N);
+    P->g64.muinv = mi64;
+    P->g32.muinv = mi32;
+  }
+  if (P->has32) {
+    float* e32 = (float*)(base + L.eps32);
+    k_to_f32<<<nb, 256, 0, s>>>(d->epsilon, e32, 3 * N);
+    P->g32.eps = e32;
+  }
+  uint8_t* mask = nullptr;
+  if (d->pec || d->pmc) {
+    mask = (uint8_t*)(base + L.mask);
+    k_mask_bits<<<nb, 256, 0, s>>>(d->pec, d->pmc, mask, N);
+  }
+  P->g64.mask = mask;
+  P->g32.mask = mask;
+  const double w2re = P->om_re * P->om_re - P->om_im * P->om_im;
+  const double w2im = 2.0 * P->om_re * P->om_im;
+  P->g64.w2 = mkc<double>(w2re, w2im);
+  P->g32.w2 = mkc<float>((float)w2re, (float)w2im);
+  P->g64.X = P->g32.X = P->X;
+  P->g64.Y = P->g32.Y = P->Y;
+  P->g64.Z = P->g32.Z = P->Z;
+  P->g64.N = P->g32.N = N;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cleanup(set_err(FDFD_ERR_CUDA, "plan set-up kernels: %s", cudaGetErrorString(e)));
+  *out = P;
+  return 0;
+}
+
+extern "C" int fdfd_plan_destroy(fdfd_plan* P) {
+  if (!P) return 0;
+  for (auto e : P->ev_pool) cudaEventDestroy(e);
+  for (auto& ge : P->graphs) cudaGraphExecDestroy(ge.exec);
+  if (P->cap) cudaStreamDestroy(P->cap);
+  cudaEventDestroy(P->ev[0]);
+  cudaEventDestroy(P->ev[1]);
+  if (P->h_poll) cudaFreeHost(P->h_poll);
+  if (P->h_state) cudaFreeHost(P->h_state);
+  delete P;
+  return 0;
+}
+
+extern "C" int fdfd_plan_set_xchunk(fdfd_plan* P, int32_t precision, int32_t xchunk) {
+  if (!P || (precision != FDFD_C128 && precision != FDFD_C64) || xchunk < 0)
+    return set_err(FDFD_ERR_ARG, "bad arguments to fdfd_plan_set_xchunk");
+  P->xc_override[precision] = xchunk;
+  for (auto& ge : P->graphs) cudaGraphExecDestroy(ge.exec);
+  P->graphs.clear();
+  return 0;
+}
+
+// ------------------------------------------------------------------ apply
+extern "C" int fdfd_apply(fdfd_plan* P, int32_t op, int32_t precision, const void* x, void* y, void* stream) {
+  if (!P || !x || !y) return set_err(FDFD_ERR_ARG, "fdfd_apply: NULL argument");
+  if (op < FDFD_OP_A0 || op > FDFD_OP_SYM_H) return set_err(FDFD_ERR_ARG, "fdfd_apply: bad op %d", op);
+  if (x == y) return set_err(FDFD_ERR_ARG, "fdfd_apply: x and y must not alias");
+  cudaStream_t s = (cudaStream_t)stream;
+  P->launches = 0;
+  RedBuf rb{nullptr, nullptr};
+  if (precision == FDFD_C128) {
+    OpApply<double> o{(const cx<double>*)x, (cx<double>*)y, op, P->g64};
+    return launch_stencil<double>(P, P->g64, 0, o, rb, s);
+  }
+  if (precision == FDFD_C64) {
+    if (!P->has32) return set_err(FDFD_ERR_ARG, "fdfd_apply: plan built without FDFD_GRID_FP32");
+    OpApply<float> o{(const cx<float>*)x, (cx<float>*)y, op, P->g32};
+    return launch_stencil<float>(P, P->g32, 1, o, rb, s);
+  }
+  return set_err(FDFD_ERR_ARG, "fdfd_apply: bad precision %d", precision);
+}
+
+// ------------------------------------------------------------------ workspaces
+// Every method keeps b (complex128) and, for its refinement loop, a complex128
+// partner of E plus eight vectors of the inner BiCGSTAB (R0 R1 V0 V1 P0 P1 T D) in
+// the inner precision.  COCG also needs r, q, P0, P1, which its breakdown
+// fallback (complex128 BiCGSTAB) reuses as R0, R1, P0, P1.
+struct SolveLayout {
+  size_t state, ticket, partials, resid, b, e2, cocg[4], inner[8], total;
+};
+
+static void solve_layout(const fdfd_plan* P, const fdfd_solve_opts* o, SolveLayout* L) {
+  const long long N = P->N;
+  const size_t c128 = align256(3 * N * sizeof(double2));
+  const size_t c64 = align256(3 * N * sizeof(float2));
+  size_t off = 0;
+  L->state = off;
+  off += align256(2 * sizeof(KState));
+  L->ticket = off;
+  off += 256;
+  L->resid = off;
+  off += 256;
+  L->partials = off;
+  off += align256((size_t)max_blocks(P) * 8 * sizeof(double));
+  L->b = off;
+  off += c128;
+  L->e2 = off;
+  off += c128;
+  if (o->method == FDFD_METHOD_COCG) {
+    for (int i = 0; i < 4; ++i) { L->cocg[i] = off; off += c128; }
+    const int reuse[8] = {0, 1, -1, -1, 2, 3, -1, -1};
+    for (int i = 0; i < 8; ++i) {
+      if (reuse[i] >= 0) { L->inner[i] = L->cocg[reuse[i]]; } else { L->inner[i] = off; off += c128; }
+    }
+  } else {
+    const size_t v = (o->method == FDFD_METHOD_MIXED) ? c64 : c128;
+    for (int i = 0; i < 4; ++i) L->cocg[i] = 0;
+    for (int i = 0; i < 8; ++i) { L->inner[i] = off; off += v; }
+  }
+  L->total = off;
+}
+
+static int check_opts(const fdfd_plan* P, const fdfd_solve_opts* o) {
+  if (!P || !o) return set_err(FDFD_ERR_ARG, "NULL plan or opts");
+  if (o->method < FDFD_METHOD_COCG || o->method > FDFD_METHOD_BICGSTAB)
+    return set_err(FDFD_ERR_ARG, "bad method %d", o->method);
+  if (o->criterion != FDFD_CRIT_TRUE && o->criterion != FDFD_CRIT_PRECOND)
+    return set_err(FDFD_ERR_ARG, "bad criterion %d", o->criterion);
+  if (o->maxiter < 0 || !(o->rtol >= 0) || !(o->atol >= 0)) return set_err(FDFD_ERR_ARG, "bad tolerances/maxiter");
+  if (o->method == FDFD_METHOD_MIXED && !P->has32)
+    return set_err(FDFD_ERR_ARG, "MIXED needs a plan built with FDFD_GRID_FP32");
+  return 0;
+}
+
+extern "C" int fdfd_solve_workspace_bytes(const fdfd_plan* P, const fdfd_solve_opts* o, size_t* bytes) {
+  TRY(check_opts(P, o));
+  if (!bytes) return set_err(FDFD_ERR_ARG, "bytes is NULL");
+  SolveLayout L;
+  solve_layout(P, o, &L);
+  *bytes = L.total;
+  return 0;
+}
+
+extern "C" int fdfd_residual_workspace_bytes(const fdfd_plan* P, size_t* bytes) {
+  if (!P || !bytes) return set_err(FDFD_ERR_ARG, "NULL argument");
+  *bytes = 512 + align256((size_t)max_blocks(P) * 8 * sizeof(double));
+  return 0;
+}
+
+static int residual_into(fdfd_plan* P, const void* E, const void* J, int adjoint, double* d_out, RedBuf rb,
+                         cudaStream_t s) {
+  OpResidual<double> o{(const cx<double>*)E, (const cx<double>*)J, P->om_re, P->om_im, adjoint, P->g64, d_out};
+  return launch_stencil<double>(P, P->g64, 0, o, rb, s);
+}
+
+extern "C" int fdfd_residual(fdfd_plan* P, const void* E, const void* J, double out[4], void* ws, size_t ws_bytes,
+                             void* stream) {
+  size_t need = 0;
+  TRY(fdfd_residual_workspace_bytes(P, &need));
+  if (!E || !J || !out || !ws) return set_err(FDFD_ERR_ARG, "fdfd_residual: NULL argument");
+  if (ws_bytes < need) return set_err(FDFD_ERR_WORKSPACE, "residual workspace too small: %zu < %zu", ws_bytes, need);
+  if (((uintptr_t)ws & 255) != 0) return set_err(FDFD_ERR_ARG, "residual workspace must be 256-byte aligned");
+  cudaStream_t s = (cudaStream_t)stream;
+  char* base = (char*)ws;
+  unsigned int* ticket = (unsigned int*)base;
+  double* d_out = (double*)(base + 256);
+  RedBuf rb{(double*)(base + 512), ticket};
+  P->launches = 0;
+  CK(cudaMemsetAsync(ticket, 0, sizeof(unsigned int), s));
+  TRY(residual_into(P, E, J, 0, d_out, rb, s));
+  CK(cudaMemcpyAsync(P->h_state, d_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  const double* h = (const double*)P->h_state;
+  for (int i = 0; i < 4; ++i) out[i] = std::sqrt(h[i]);
+  return 0;
+}
+
+// ------------------------------------------------------------------ iteration driver
+// Runs `body` (which enqueues one batch of iterations) until the device state
+// leaves ST_RUNNING.  Batches are enqueued one ahead of the convergence check, so
+// the GPU never idles while the host polls; kernels of a batch that starts after
+// convergence return at once (they test the status first).
+template <class Body>
+static int drive(fdfd_plan* P, KState* d_st, int chunk, int maxiter, cudaStream_t s, Body body) {
+  int* hp = P->h_poll;
+  const int max_batches = maxiter / chunk + 3;
+  int b = 0;
+  for (;;) {
+    TRY(body());
+    CK(cudaMemcpyAsync(hp + 4 * (b & 1), &d_st->crit, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaEventRecord(P->ev[b & 1], s));
+    if (b > 0) {
+      CK(cudaEventSynchronize(P->ev[(b - 1) & 1]));
+      if (hp[4 * ((b - 1) & 1) + 3] != ST_RUNNING) break;
+    }
+    ++b;
+    if (b >= max_batches) break;
+  }
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+// Capture `enqueue` (one batch) as a CUDA graph on the private stream, cached by key.
+template <class Enq>
+static int graph_batch(fdfd_plan* P, int kind, const void* ka, const void* kb, int chunk, cudaStream_t s,
+                       Enq enqueue) {
+  for (auto& ge : P->graphs) {
+    if (ge.kind == kind && ge.a == ka && ge.b == kb && ge.chunk == chunk) {
+      CK(cudaGraphLaunch(ge.exec, s));
+      return 0;
+    }
+  }
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(P->cap, cudaStreamCaptureModeThreadLocal));
+  const int saved = P->launches;
+  int rc = enqueue(P->cap);
+  P->launches = saved;
+  cudaError_t e = cudaStreamEndCapture(P->cap, &g);
+  if (rc != 0) return rc;
+  if (e != cudaSuccess) return set_err(FDFD_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+  cudaGraphExec_t ex;
+  e = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return set_err(FDFD_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+  P->graphs.push_back({kind, ka, kb, chunk, ex});
+  CK(cudaGraphLaunch(ex, s));
+  return 0;
+}
+
+static KState make_state(const fdfd_solve_opts* o, int crit, int maxiter, double* hist) {
+  KState h;
+  memset(&h, 0, sizeof(h));
+  h.crit = crit;
+  h.maxiter = maxiter;
+  h.rtol = o->rtol;
+  h.atol = o->atol;
+  h.hist = hist;
+  h.status = ST_RUNNING;
+  return h;
+}
+
+struct SolveCtx {
+  fdfd_plan* P;
+  const fdfd_solve_opts* o;
+  cudaStream_t s;
+  void* ws;
+  KState* st;      // outer state
+  KState* st_in;   // inner state
+  RedBuf rb;
+  cx<double>* b;
+  cx<double>* x;   // the caller's E
+  cx<double>* e2;  // partner of E for the refinement ping-pong
+  int crit, chunk;
+  double tol2;     // on the monitored norm^2
+  double bnorm;    // |b|
+  int iters, outer, status;
+};
+
+static double monitored(const KState& h, int crit) { return crit == 0 ? h.rr : (crit == 1 ? h.rr_pc : h.rr_w2); }
+
+// Refinement loop: r = b - A0 E in complex128 (exact criterion), then an inner
+// BiCGSTAB in precision RI on A0 d = r / |b| to a relative reduction eta, and
+// E += |b| d; repeated until the criterion holds.  E starts from the current
+// content of ctx.x; the result ends in ctx.x.
+template <typename RI>
+static int refine_loop(SolveCtx& c, const Geo<RI>& gi, int prec, BsBufs B, double eta, int max_outer, int kind) {
+  fdfd_plan* P = c.P;
+  cudaStream_t s = c.s;
+  const long long N = P->N;
+  const size_t vb = 3 * N * sizeof(cx<RI>);
+  const double rscale = c.bnorm > 0 ? 1.0 / c.bnorm : 1.0;
+  cx<double>* Ecur = c.x;
+  cx<double>* Enext = c.e2;
+  cx<RI>* D = (cx<RI>*)B.x;
+  bool have_d = false;
+  int local_outer = 0;
+  for (;;) {
+    // the shadow seed is baked into captured graphs, which are keyed by local_outer % 8
+    const unsigned long long seed = 0x5eed5eedULL + 0x9e3779b97f4a7c15ULL * (unsigned long long)(local_outer % 8);
+    OpRefine<RI> rf{Ecur, have_d ? D : nullptr, Enext, c.b, (cx<RI>*)B.R[0], c.bnorm, rscale, N, seed, c.st};
+    TRY(launch_stencil<double>(P, P->g64, 0, rf, c.rb, s));
+    std::swap(Ecur, Enext);
+    CK(cudaMemcpyAsync(P->h_state, c.st, sizeof(KState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const KState ho = *P->h_state;
+    const double mon = monitored(ho, c.crit);
+    if (!std::isfinite(mon)) { c.status = ST_NONFINITE; break; }
+    if (mon <= c.tol2) { c.status = ST_CONVERGED; break; }
+    if (local_outer >= max_outer || c.iters >= c.o->maxiter) { c.status = ST_MAXITER; break; }
+    ++local_outer;
+    ++c.outer;
+    KState hi = make_state(c.o, 0, std::max(1, c.o->maxiter - c.iters), nullptr);
+    hi.rho = {ho.extra[0], ho.extra[1]};
+    hi.rr = ho.extra[2];
+    hi.bb = ho.extra[2];
+    hi.tol2 = eta * eta * ho.extra[2];
+    *P->h_state = hi;
+    CK(cudaMemcpyAsync(c.st_in, P->h_state, sizeof(KState), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(D, 0, vb, s));
+    KState* sti = c.st_in;
+    RedBuf rb = c.rb;
+    const int chunk = c.chunk;
+    auto enqueue = [&, seed](cudaStream_t ss) -> int {
+      for (int it = 0; it < chunk; ++it) {
+        {
+          ProfScope ps(P, 2, ss);
+          OpBsP<RI> pp{B, N, seed, sti};
+          TRY(launch_stencil<RI>(P, gi, prec, pp, rb, ss));
+        }
+        {
+          ProfScope ps(P, 3, ss);
+          OpBsS<RI> sp{B, N, seed, sti};
+          TRY(launch_stencil<RI>(P, gi, prec, sp, rb, ss));
+        }
+      }
+      return 0;
+    };
+    // the shadow seed is baked into the batch, so graphs are keyed by it too
+    TRY(drive(P, sti, chunk, hi.maxiter, s, [&]() -> int {
+      if (c.o->use_graph && !P->profiling) {
+        P->launches += 2 * chunk;
+        return graph_batch(P, kind + 16 * (local_outer % 8), c.ws, c.x, chunk, s, enqueue);
+      }
+      return enqueue(s);
+    }));
+    OpBsFinal<RI> fin{B, N, sti};
+    TRY(launch_point<RI>(P, gi, prec, fin, rb, s));
+    CK(cudaMemcpyAsync(P->h_state, sti, sizeof(KState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    c.iters += P->h_state->iter;
+    if (P->h_state->status == ST_NONFINITE) { c.status = ST_NONFINITE; break; }
+    have_d = true;
+  }
+  if (Ecur != c.x) CK(cudaMemcpyAsync(c.x, Ecur, 3 * N * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+  return 0;
+}
+
+// ------------------------------------------------------------------ solve
+extern "C" int fdfd_solve(fdfd_plan* P, const fdfd_solve_opts* o, const void* J, void* E, void* ws,
+                          size_t ws_bytes, fdfd_solve_info* info, void* stream) {
+  TRY(check_opts(P, o));
+  if (!J || !E || !ws) return set_err(FDFD_ERR_ARG, "fdfd_solve: NULL J, E or workspace");
+  if (((uintptr_t)ws & 255) != 0) return set_err(FDFD_ERR_ARG, "solve workspace must be 256-byte aligned");
+  SolveLayout L;
+  solve_layout(P, o, &L);
+  if (ws_bytes < L.total) return set_err(FDFD_ERR_WORKSPACE, "solve workspace too small: %zu < %zu", ws_bytes, L.total);
+  cudaStream_t s = (cudaStream_t)stream;
+  P->launches = 0;
+  P->profiling = o->profile != 0;
+  P->ev_marks.clear();
+  P->ev_used = 0;
+  char* base = (char*)ws;
+  const long long N = P->N;
+  const size_t vbytes128 = 3 * N * sizeof(double2);
+
+  SolveCtx c;
+  c.P = P;
+  c.o = o;
+  c.s = s;
+  c.ws = ws;
+  c.st = (KState*)(base + L.state);
+  c.st_in = c.st + 1;
+  unsigned int* ticket = (unsigned int*)(base + L.ticket);
+  double* d_res = (double*)(base + L.resid);
+  c.rb = RedBuf{(double*)(base + L.partials), ticket};
+  c.b = (cx<double>*)(base + L.b);
+  c.x = (cx<double>*)E;
+  c.e2 = (cx<double>*)(base + L.e2);
+  c.crit = (o->criterion == FDFD_CRIT_PRECOND) ? 1 : (o->adjoint ? 2 : 0);
+  c.chunk = o->chunk > 0 ? o->chunk : 16;
+  c.iters = 0;
+  c.outer = 0;
+  c.status = ST_RUNNING;
+  const int maxiter = o->maxiter;
+  BsBufs B;
+  B.R[0] = base + L.inner[0];
+  B.R[1] = base + L.inner[1];
+  B.V[0] = base + L.inner[2];
+  B.V[1] = base + L.inner[3];
+  B.P[0] = base + L.inner[4];
+  B.P[1] = base + L.inner[5];
+  B.T = base + L.inner[6];
+  B.x = base + L.inner[7];
+
+  KState h = make_state(o, c.crit, maxiter, o->history);
+  *P->h_state = h;
+  CK(cudaMemsetAsync(ticket, 0, sizeof(unsigned int), s));
+  CK(cudaMemcpyAsync(c.st, P->h_state, sizeof(KState), cudaMemcpyHostToDevice, s));
+  // right-hand side (and guess) in the solve space; E holds the iterate
+  {
+    OpRhs<double> op{(const cx<double>*)J, o->has_guess ? (const cx<double>*)E : nullptr, c.b, c.x,
+                     P->om_re, P->om_im, o->adjoint, P->g64.mask, N, c.st};
+    TRY(launch_point<double>(P, P->g64, 0, op, c.rb, s));
+  }
+  if (!o->has_guess) CK(cudaMemsetAsync(E, 0, vbytes128, s));
+  CK(cudaMemcpyAsync(P->h_state, c.st, sizeof(KState), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  {
+    const KState hb = *P->h_state;
+    const double bbm = c.crit == 0 ? hb.bb : (c.crit == 1 ? hb.bb_pc : hb.bb_w2);
+    c.tol2 = std::max(o->rtol * o->rtol * bbm, o->atol * o->atol);
+    c.bnorm = std::sqrt(hb.bb);
+  }
+
+  if (o->method == FDFD_METHOD_COCG) {
+    cx<double>* r = (cx<double>*)(base + L.cocg[0]);
+    cx<double>* q = (cx<double>*)(base + L.cocg[1]);
+    cx<double>* P0 = (cx<double>*)(base + L.cocg[2]);
+    cx<double>* P1 = (cx<double>*)(base + L.cocg[3]);
+    CK(cudaMemsetAsync(P0, 0, vbytes128, s));
+    {
+      OpCocgInit<double> op{c.b, o->has_guess ? c.x : nullptr, r, N, c.st};
+      TRY(launch_stencil<double>(P, P->g64, 0, op, c.rb, s));
+    }
+    KState* st = c.st;
+    RedBuf rb = c.rb;
+    const int chunk = c.chunk;
+    cx<double>* x = c.x;
+    auto enqueue = [&](cudaStream_t ss) -> int {
+      for (int it = 0; it < chunk; ++it) {
+        {
+          ProfScope ps(P, 0, ss);
+          OpCocgA<double> a{r, P0, P1, x, q, N, st};
+          TRY(launch_stencil<double>(P, P->g64, 0, a, rb, ss));
+        }
+        {
+          ProfScope ps(P, 1, ss);
+          OpCocgB<double> bb{r, q, N, st};
+          TRY(launch_point<double>(P, P->g64, 0, bb, rb, ss));
+        }
+      }
+      return 0;
+    };
+    if (maxiter > 0) {
+      TRY(drive(P, st, chunk, maxiter, s, [&]() -> int {
+        if (o->use_graph && !P->profiling) {
+          P->launches += 2 * chunk;
+          return graph_batch(P, 0, ws, E, chunk, s, enqueue);
+        }
+        return enqueue(s);
+      }));
+    }
+    OpCocgFinal<double> fin{P0, P1, x, N, st};
+    TRY(launch_point<double>(P, P->g64, 0, fin, rb, s));
+    CK(cudaMemcpyAsync(P->h_state, st, sizeof(KState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    c.iters = P->h_state->iter;
+    c.status = P->h_state->status;
+    if (c.status == ST_BREAKDOWN || c.status == ST_NONFINITE) {
+      // COCG broke down (the unconjugated form cancelled): continue from the
+      // current iterate with complex128 BiCGSTAB inside the refinement loop.
+      if (c.status == ST_NONFINITE) CK(cudaMemsetAsync(E, 0, vbytes128, s));
+      c.status = ST_RUNNING;
+      TRY(refine_loop<double>(c, P->g64, 0, B, 1e-10, 64, 2));
+    }
+  } else if (o->method == FDFD_METHOD_MIXED) {
+    const double eta = o->inner_rtol > 0 ? o->inner_rtol : 1e-2;
+    const int max_outer = o->max_outer > 0 ? o->max_outer : 64;
+    TRY(refine_loop<float>(c, P->g32, 1, B, eta, max_outer, 1));
+  } else {
+    const double eta = o->inner_rtol > 0 ? o->inner_rtol : 1e-10;
+    const int max_outer = o->max_outer > 0 ? o->max_outer : 64;
+    TRY(refine_loop<double>(c, P->g64, 0, B, eta, max_outer, 2));
+  }
+
+  if (o->adjoint) {
+    OpAdjPost<double> post{c.x, N};
+    TRY(launch_point<double>(P, P->g64, 0, post, c.rb, s));
+  }
+  // final FP64 check against the unmasked right-hand side
+  TRY(residual_into(P, E, J, o->adjoint, d_res, c.rb, s));
+  CK(cudaMemcpyAsync(P->h_state, d_res, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  double hr[4];
+  memcpy(hr, P->h_state, sizeof(hr));
+  if (info) {
+    for (int k = 0; k < 4; ++k) {
+      info->kernel_ms[k] = 0.0;
+      info->kernel_count[k] = 0;
+    }
+    if (P->profiling) prof_collect(P, info->kernel_ms, info->kernel_count);
+    info->status = c.status;
+    info->iterations = c.iters;
+    info->outer_iterations = c.outer;
+    info->kernel_launches = P->launches;
+    info->residual = hr[2] > 0 ? std::sqrt(hr[0] / hr[2]) : std::sqrt(hr[0]);
+    info->residual_pc = hr[3] > 0 ? std::sqrt(hr[1] / hr[3]) : std::sqrt(hr[1]);
+  }
+  P->profiling = false;
+  return c.status == ST_CONVERGED ? 0 : c.status;
+}

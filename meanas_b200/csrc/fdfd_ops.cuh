@@ -1,0 +1,848 @@
+// Loaders/epilogues plugged into the stencil and pointwise engines of fdfd_device.cuh.
+//
+// Krylov methods (all in the E-space, i.e. on A0 itself):
+//
+//  * COCG on A0 with the bilinear form <u, v> = sum(u * W * v), W = p^2 the
+//    symmetriser weights of meanas/fdfd/operators.py:99-123.  With x = Pl E this
+//    is exactly COCG on the symmetrised system Pl A0 Pr x = Pl b0 that
+//    meanas/fdfd/solvers.py:116-134 builds (W A0 is complex symmetric), but it
+//    needs no square roots and no Pl/Pr vectors.  One stencil pass per iteration
+//    forms p = r + beta p_old, applies q = A0 p, applies the deferred update
+//    x += alpha_old p_old and reduces p^T W q; a pointwise pass updates
+//    r -= alpha q and reduces r^T W r, |r|^2 and sum |W| |r|^2.
+//
+//  * BiCGSTAB with a hashed pseudo-random shadow vector (no storage), used in
+//    complex64 as the inner solver of the mixed-precision refinement.  Two stencil
+//    passes per iteration: P (r, p, x updates + v = A0 p) and S (s = r - alpha v,
+//    t = A0 s).  Hermitian shadow products keep it stable in single precision,
+//    which the unconjugated bilinear form of COCG is not on PML problems.
+//
+//  * Refinement pass (complex128): E_new = E_old + scale * d, r = b - A0 E_new,
+//    writes the scaled complex64 residual for the next inner solve.
+#pragma once
+#include "fdfd_device.cuh"
+
+namespace fdfd {
+
+enum SolveStatus : int {
+  ST_RUNNING = 0,
+  ST_CONVERGED = 1,
+  ST_MAXITER = 2,
+  ST_BREAKDOWN = 3,
+  ST_NONFINITE = 4,
+};
+
+// COCG (near) breakdown: the unconjugated form r^T W r (or p^T W q) has cancelled to
+// below this fraction of its magnitude bound.  Converging PML runs stay above ~1e-10.
+constexpr double BREAKDOWN_RATIO = 1e-14;
+
+// FP64 scalar state of one Krylov sequence (device memory).
+struct KState {
+  dcx rho, sigma, alpha, beta, omega;
+  double rr;       // |r|^2 (recurrence residual)
+  double rr_pc;    // sum |W| |r|^2
+  double rr_w2;    // sum |W|^2 |r|^2
+  double bb;       // |b|^2
+  double bb_pc;    // sum |W| |b|^2
+  double bb_w2;    // sum |W|^2 |b|^2
+  double rtol, atol;
+  double tol2;     // stop when monitored norm^2 <= tol2
+  double b0b0;     // |b0|^2 of the unmasked right-hand side
+  double extra[4];
+  int crit;        // 0: monitor rr, 1: monitor rr_pc, 2: monitor rr_w2
+  int iter, maxiter, status;
+  int pending;     // an x update is still owed (deferred update)
+  int pad;
+  double* hist;    // relative residual history (length maxiter + 1) or null
+};
+
+__device__ __forceinline__ int ld_status(const KState* st) {
+  return *((volatile const int*)&st->status);
+}
+
+__device__ __forceinline__ dcx ld_dcx(const dcx* p) {
+  return {__ldcg(&p->re), __ldcg(&p->im)};
+}
+
+// The norm^2 a criterion watches, for the residual and for the right-hand side.
+__device__ __forceinline__ double monitored_rr(const KState* st) {
+  return st->crit == 0 ? st->rr : (st->crit == 1 ? st->rr_pc : st->rr_w2);
+}
+__device__ __forceinline__ double monitored_bb(const KState* st) {
+  return st->crit == 0 ? st->bb : (st->crit == 1 ? st->bb_pc : st->bb_w2);
+}
+
+__device__ __forceinline__ void check_progress(KState* st, double monitored, bool finite_ok) {
+  const double bbm = monitored_bb(st);
+  const double rel = bbm > 0 ? sqrt(monitored / bbm) : 0.0;
+  if (st->hist) st->hist[st->iter] = rel;
+  if (!finite_ok || !isfinite(monitored)) {
+    st->status = ST_NONFINITE;
+  } else if (monitored <= st->tol2) {
+    st->status = ST_CONVERGED;
+  } else if (st->iter >= st->maxiter) {
+    st->status = ST_MAXITER;
+  }
+}
+
+// |W| for the three components (magnitudes multiply, so no square root per cell).
+template <typename R>
+__device__ __forceinline__ void absW3(const cx<R> W[3], R a[3]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) a[c] = sqrt(cabs2(W[c]));
+}
+
+// ------------------------------------------------------------------ plain operator
+// y = post( A0 pre(x) ):  modes
+//   0: A0
+//   1: Pl A0 Pr                    (the symmetrised operator of generic())
+//   2: (Pl A0 Pr)^H = conj(Pl A0 Pr conj(x))
+// Pl = principal sqrt of p^2, Pr = 1/Pl (meanas/fdfd/operators.py:120-122).
+__device__ __forceinline__ dcx csqrt_principal(dcx z) {
+  // sqrt of a complex number, principal branch (Re >= 0; branch cut on the
+  // negative real axis with the sign of the imaginary part kept).
+  const double a = fabs(z.re), b = fabs(z.im);
+  if (a == 0.0 && b == 0.0) return {0.0, z.im};
+  const double t = sqrt(0.5 * (hypot(a, b) + a));
+  if (z.re >= 0.0) return {t, z.im / (2.0 * t)};
+  return {b / (2.0 * t), copysign(t, z.im)};
+}
+
+template <typename R>
+struct OpApply {
+  static constexpr int NRED = 0;
+  static constexpr bool NEEDS_W = true;
+  const cx<R>* x;
+  cx<R>* y;
+  int mode;
+  Geo<R> g;
+  __device__ bool skip() const { return false; }
+  __device__ void prepare() {}
+  __device__ cx<R> pl_at(int c, long long idx) const {
+    const long long N = g.N;
+    const long long cell = idx - c * N;
+    const long long YZ = (long long)g.Y * g.Z;
+    const int i = (int)(cell / YZ);
+    const int j = (int)((cell / g.Z) % g.Y);
+    const int k = (int)(cell % g.Z);
+    cx<R> p2;
+    if (c == 0) p2 = g.dxe[0][i] * g.dxh[1][j] * g.dxh[2][k];
+    else if (c == 1) p2 = g.dxh[0][i] * g.dxe[1][j] * g.dxh[2][k];
+    else p2 = g.dxh[0][i] * g.dxh[1][j] * g.dxe[2][k];
+    dcx s = csqrt_principal({(double)p2.re, (double)p2.im});
+    return mkc<R>((R)s.re, (R)s.im);
+  }
+  __device__ cx<R> load(int c, long long idx) const {
+    cx<R> v = x[idx];
+    if (mode == 2) v = cconj(v);
+    if (mode >= 1) {
+      const cx<R> pl = pl_at(c, idx);
+      // Pr = 1 / Pl
+      const R d = cabs2(pl);
+      const cx<R> pr = mkc<R>(pl.re / d, -pl.im / d);
+      v = v * pr;
+    }
+    return v;
+  }
+  __device__ void own(long long cell, int, int, int, const cx<R>*, const cx<R> yv[3], const cx<R>*,
+                      double*) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long idx = c * g.N + cell;
+      cx<R> v = yv[c];
+      if (mode >= 1) v = pl_at(c, idx) * v;
+      if (mode == 2) v = cconj(v);
+      y[idx] = v;
+    }
+  }
+  __device__ void finish(const double*) const {}
+};
+
+// ------------------------------------------------------------------ right-hand sides
+// b = pe * (-i omega J)                       (forward, meanas/fdfd/solvers.py:115)
+// b = W^-1 conj(pe * (-i omega J))            (adjoint: A0^H E = b0  <=>  A0 y = W^-1 conj(b0),
+//                                              E = conj(W y); W A0 is symmetric)
+// Also maps an initial guess into the same space (x0 = E or W^-1 conj(E)) and
+// reduces |b0|^2 for the unmasked true residual.
+template <typename R>
+struct OpRhs {
+  static constexpr int NRED = 4;
+  static constexpr bool NEEDS_W = true;
+  const cx<R>* J;
+  const cx<R>* E0;  // optional guess
+  cx<R>* b;
+  cx<R>* x0;        // written when E0 given
+  double om_re, om_im;
+  int adjoint;
+  const uint8_t* mask;
+  long long N;
+  KState* st;
+  __device__ bool skip() const { return false; }
+  __device__ void prepare() {}
+  __device__ void point(long long cell, int, int, int, const cx<R> W[3], double* acc) const {
+    const uint8_t m = mask ? mask[cell] : (uint8_t)0;
+    R aW[3];
+    absW3<R>(W, aW);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long idx = c * N + cell;
+      const cx<R> j = J[idx];
+      // -i * omega * J
+      const cx<R> b0 = mkc<R>((R)(om_im * j.re + om_re * j.im), (R)(om_im * j.im - om_re * j.re));
+      acc[0] += (double)cabs2(b0);
+      cx<R> bv = (m & (1u << c)) ? czero<R>() : b0;
+      cx<R> wi = mkc<R>(R(1), R(0));
+      if (adjoint) {
+        const R d = cabs2(W[c]);
+        wi = mkc<R>(W[c].re / d, -W[c].im / d);
+        bv = wi * cconj(bv);
+      }
+      b[idx] = bv;
+      const double bb = (double)cabs2(bv);
+      acc[1] += bb;
+      acc[2] += (double)aW[c] * bb;
+      acc[3] += (double)aW[c] * (double)aW[c] * bb;
+      if (E0) {
+        cx<R> e = E0[idx];
+        if (adjoint) e = wi * cconj(e);
+        x0[idx] = e;
+      }
+    }
+  }
+  __device__ void finish(const double* s) const {
+    st->b0b0 = s[0];
+    st->bb = s[1];
+    st->bb_pc = s[2];
+    st->bb_w2 = s[3];
+    const double bbm = monitored_bb(st);
+    st->tol2 = fmax(st->rtol * st->rtol * bbm, st->atol * st->atol);
+  }
+};
+
+// E = conj(W y) in place (adjoint solution back-transform).
+template <typename R>
+struct OpAdjPost {
+  static constexpr int NRED = 0;
+  static constexpr bool NEEDS_W = true;
+  cx<R>* x;
+  long long N;
+  __device__ bool skip() const { return false; }
+  __device__ void prepare() {}
+  __device__ void point(long long cell, int, int, int, const cx<R> W[3], double*) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long idx = c * N + cell;
+      x[idx] = cconj(W[c] * x[idx]);
+    }
+  }
+  __device__ void finish(const double*) const {}
+};
+
+// ------------------------------------------------------------------ COCG
+// init: r = b - A0 x0 (x0 may be zero); reduces r^T W r, |r|^2, sum|W||r|^2, sum|W|^2|r|^2
+template <typename R>
+struct OpCocgInit {
+  static constexpr int NRED = 5;
+  static constexpr bool NEEDS_W = true;
+  const cx<R>* b;
+  const cx<R>* x;  // may be null (zero guess)
+  cx<R>* r;
+  long long N;
+  KState* st;
+  __device__ bool skip() const { return false; }
+  __device__ void prepare() {}
+  __device__ cx<R> load(int, long long idx) const { return x ? x[idx] : czero<R>(); }
+  __device__ void own(long long cell, int, int, int, const cx<R>*, const cx<R> y[3], const cx<R> W[3],
+                      double* acc) const {
+    R aW[3];
+    absW3<R>(W, aW);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long idx = c * N + cell;
+      const cx<R> rv = b[idx] - y[c];
+      r[idx] = rv;
+      const cx<R> wr = W[c] * rv;
+      acc[0] += (double)wr.re * (double)rv.re - (double)wr.im * (double)rv.im;
+      acc[1] += (double)wr.re * (double)rv.im + (double)wr.im * (double)rv.re;
+      const double r2 = (double)cabs2(rv);
+      acc[2] += r2;
+      acc[3] += (double)aW[c] * r2;
+      acc[4] += (double)aW[c] * (double)aW[c] * r2;
+    }
+  }
+  __device__ void finish(const double* s) const {
+    st->rho = {s[0], s[1]};
+    st->rr = s[2];
+    st->rr_pc = s[3];
+    st->rr_w2 = s[4];
+    st->beta = {0.0, 0.0};
+    st->alpha = {0.0, 0.0};
+    st->iter = 0;
+    st->pending = 0;
+    st->status = ST_RUNNING;
+    check_progress(st, monitored_rr(st), dfinite(st->rho));
+    if (st->status == ST_MAXITER) st->status = ST_RUNNING;  // maxiter == 0 is handled on the host
+    if (st->status == ST_RUNNING && dabs(st->rho) <= BREAKDOWN_RATIO * s[3]) st->status = ST_BREAKDOWN;
+  }
+};
+
+// p = r + beta p_old ; x += alpha p_old (deferred) ; q = A0 p ; sigma = p^T W q
+template <typename R>
+struct OpCocgA {
+  static constexpr int NRED = 4;
+  static constexpr bool NEEDS_W = true;
+  const cx<R>* r;
+  cx<R>* P0;
+  cx<R>* P1;
+  cx<R>* x;
+  cx<R>* q;
+  long long N;
+  KState* st;
+  // per-thread
+  const cx<R>* p_old;
+  cx<R>* p_new;
+  cx<R> beta, alpha;
+  bool upd;
+  __device__ bool skip() const { return ld_status(st) != ST_RUNNING; }
+  __device__ void prepare() {
+    const int k = __ldcg(&st->iter);
+    p_old = (k & 1) ? P1 : P0;
+    p_new = (k & 1) ? P0 : P1;
+    beta = from_d<R>(ld_dcx(&st->beta));
+    alpha = from_d<R>(ld_dcx(&st->alpha));
+    upd = __ldcg(&st->pending) != 0;
+  }
+  __device__ cx<R> load(int, long long idx) const { return caxpy(beta, p_old[idx], r[idx]); }
+  __device__ void own(long long cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R> W[3],
+                      double* acc) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long idx = c * N + cell;
+      if (upd) x[idx] = caxpy(alpha, p_old[idx], x[idx]);
+      p_new[idx] = u[c];
+      q[idx] = y[c];
+      const cx<R> wp = W[c] * u[c];
+      acc[0] += (double)wp.re * (double)y[c].re - (double)wp.im * (double)y[c].im;
+      acc[1] += (double)wp.re * (double)y[c].im + (double)wp.im * (double)y[c].re;
+      const double aw = (double)sqrt(cabs2(W[c]));
+      acc[2] += aw * (double)cabs2(u[c]);
+      acc[3] += aw * (double)cabs2(y[c]);
+    }
+  }
+  __device__ void finish(const double* s) const {
+    const dcx sigma = {s[0], s[1]};
+    st->sigma = sigma;
+    st->pending = 0;
+    if (!dfinite(sigma)) {
+      st->status = ST_NONFINITE;
+      return;
+    }
+    // |p^T W q| <= ||p||_|W| ||q||_|W|; a ratio below 1e-14 is a (near) breakdown
+    if (dabs(sigma) <= BREAKDOWN_RATIO * sqrt(s[2] * s[3])) {
+      st->status = ST_BREAKDOWN;
+      return;
+    }
+    st->alpha = ddiv(st->rho, sigma);
+  }
+};
+
+// r -= alpha q ; rho_new = r^T W r ; |r|^2 ; sum|W||r|^2 ; sum|W|^2|r|^2 ; beta = rho_new / rho
+template <typename R>
+struct OpCocgB {
+  static constexpr int NRED = 5;
+  static constexpr bool NEEDS_W = true;
+  cx<R>* r;
+  const cx<R>* q;
+  long long N;
+  KState* st;
+  cx<R> malpha;
+  __device__ bool skip() const { return ld_status(st) != ST_RUNNING; }
+  __device__ void prepare() {
+    const dcx a = ld_dcx(&st->alpha);
+    malpha = mkc<R>((R)(-a.re), (R)(-a.im));
+  }
+  __device__ void point(long long cell, int, int, int, const cx<R> W[3], double* acc) const {
+    R aW[3];
+    absW3<R>(W, aW);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long idx = c * N + cell;
+      const cx<R> rv = caxpy(malpha, q[idx], r[idx]);
+      r[idx] = rv;
+      const cx<R> wr = W[c] * rv;
+      acc[0] += (double)wr.re * (double)rv.re - (double)wr.im * (double)rv.im;
+      acc[1] += (double)wr.re * (double)rv.im + (double)wr.im * (double)rv.re;
+      const double r2 = (double)cabs2(rv);
+      acc[2] += r2;
+      acc[3] += (double)aW[c] * r2;
+      acc[4] += (double)aW[c] * (double)aW[c] * r2;
+    }
+  }
+  __device__ void finish(const double* s) const {
+    const dcx rho_new = {s[0], s[1]};
+    st->rr = s[2];
+    st->rr_pc = s[3];
+    st->rr_w2 = s[4];
+    st->iter += 1;
+    const bool ok = dfinite(rho_new);
+    st->pending = ok ? 1 : 0;
+    check_progress(st, monitored_rr(st), ok);
+    if (st->status != ST_RUNNING) {
+      st->rho = rho_new;
+      return;
+    }
+    // |r^T W r| <= sum |W||r|^2; a ratio below 1e-14 is a (near) breakdown
+    if (dabs(rho_new) <= BREAKDOWN_RATIO * s[3]) {
+      st->status = ST_BREAKDOWN;
+      return;
+    }
+    st->beta = ddiv(rho_new, st->rho);
+    st->rho = rho_new;
+  }
+};
+
+// x += alpha * p_last if an update is owed (after the loop stops).
+template <typename R>
+struct OpCocgFinal {
+  static constexpr int NRED = 0;
+  static constexpr bool NEEDS_W = false;
+  cx<R>* P0;
+  cx<R>* P1;
+  cx<R>* x;
+  long long N;
+  KState* st;
+  const cx<R>* p;
+  cx<R> alpha;
+  bool upd;
+  __device__ bool skip() const { return false; }
+  __device__ void prepare() {
+    const int k = __ldcg(&st->iter);
+    p = (k & 1) ? P1 : P0;
+    alpha = from_d<R>(ld_dcx(&st->alpha));
+    upd = __ldcg(&st->pending) != 0;
+  }
+  __device__ void point(long long cell, int, int, int, const cx<R>*, double*) const {
+    if (!upd) return;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long idx = c * N + cell;
+      x[idx] = caxpy(alpha, p[idx], x[idx]);
+    }
+  }
+  __device__ void finish(const double*) const {}
+};
+
+// ------------------------------------------------------------------ BiCGSTAB
+// Shadow vector: a fixed pseudo-random complex vector derived from the element
+// index (splitmix64), so it costs no memory traffic.
+__device__ __forceinline__ dcx shadow_d(long long idx, unsigned long long seed) {
+  unsigned long long z = (unsigned long long)idx * 0x9e3779b97f4a7c15ull + seed;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  z ^= z >> 31;
+  const double a = (double)(unsigned)(z & 0xffffffffu) * (1.0 / 4294967296.0) - 0.5;
+  const double b = (double)(unsigned)(z >> 32) * (1.0 / 4294967296.0) - 0.5;
+  return {a, b};
+}
+template <typename R>
+__device__ __forceinline__ cx<R> shadow(long long idx, unsigned long long seed) {
+  dcx d = shadow_d(idx, seed);
+  return mkc<R>((R)d.re, (R)d.im);
+}
+// conj(a) * b accumulated in FP64
+template <typename R>
+__device__ __forceinline__ void acc_cdot(double* acc, cx<R> a, cx<R> b) {
+  acc[0] += (double)a.re * (double)b.re + (double)a.im * (double)b.im;
+  acc[1] += (double)a.re * (double)b.im - (double)a.im * (double)b.re;
+}
+
+struct BsBufs {
+  void* R[2];
+  void* V[2];
+  void* P[2];
+  void* T;
+  void* x;
+};
+
+// P pass (iteration k, buffers old = k&1, new = (k+1)&1):
+//   s = r_old - alpha v_old ; r = s - omega t ; p = r + beta (p_old - omega v_old)
+//   x += alpha p_old + omega s ; v = A0 p ; sigma = (rh, v) ; |r|^2
+template <typename R>
+struct OpBsP {
+  static constexpr int NRED = 3;
+  static constexpr bool NEEDS_W = false;
+  BsBufs B;
+  long long N;
+  unsigned long long seed;
+  KState* st;
+  const cx<R>* ro;
+  const cx<R>* vo;
+  const cx<R>* po;
+  const cx<R>* t;
+  cx<R>* rn;
+  cx<R>* vn;
+  cx<R>* pn;
+  cx<R>* x;
+  cx<R> alpha, omega, beta, malpha, momega;
+  bool upd;
+  __device__ bool skip() const { return ld_status(st) != ST_RUNNING; }
+  __device__ void prepare() {
+    const int k = __ldcg(&st->iter);
+    const int o = k & 1, n = o ^ 1;
+    ro = (const cx<R>*)B.R[o];
+    vo = (const cx<R>*)B.V[o];
+    po = (const cx<R>*)B.P[o];
+    rn = (cx<R>*)B.R[n];
+    vn = (cx<R>*)B.V[n];
+    pn = (cx<R>*)B.P[n];
+    t = (const cx<R>*)B.T;
+    x = (cx<R>*)B.x;
+    upd = __ldcg(&st->pending) != 0;
+    if (upd) {
+      alpha = from_d<R>(ld_dcx(&st->alpha));
+      omega = from_d<R>(ld_dcx(&st->omega));
+    } else {
+      alpha = czero<R>();
+      omega = czero<R>();
+    }
+    beta = upd ? from_d<R>(ld_dcx(&st->beta)) : czero<R>();
+    malpha = mkc<R>(-alpha.re, -alpha.im);
+    momega = mkc<R>(-omega.re, -omega.im);
+  }
+  __device__ cx<R> load(int, long long idx) const {
+    if (!upd) return ro[idx];
+    const cx<R> v = vo[idx];
+    const cx<R> s = caxpy(malpha, v, ro[idx]);
+    const cx<R> r = caxpy(momega, t[idx], s);
+    return caxpy(beta, caxpy(momega, v, po[idx]), r);
+  }
+  __device__ void own(long long cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R>*,
+                      double* acc) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long idx = c * N + cell;
+      cx<R> r;
+      if (upd) {
+        const cx<R> s = caxpy(malpha, vo[idx], ro[idx]);
+        r = caxpy(momega, t[idx], s);
+        x[idx] = caxpy(omega, s, caxpy(alpha, po[idx], x[idx]));
+      } else {
+        r = ro[idx];
+      }
+      rn[idx] = r;
+      pn[idx] = u[c];
+      vn[idx] = y[c];
+      acc_cdot<R>(acc, shadow<R>(idx, seed), y[c]);
+      acc[2] += (double)cabs2(r);
+    }
+  }
+  __device__ void finish(const double* s) const {
+    const dcx sigma = {s[0], s[1]};
+    st->sigma = sigma;
+    st->rr = s[2];
+    st->pending = 0;
+    if (!dfinite(sigma) || !isfinite(s[2])) {
+      st->status = ST_NONFINITE;
+      return;
+    }
+    if (dabs(sigma) <= 1e-300 || dabs(st->rho) <= 1e-300) {
+      st->status = ST_BREAKDOWN;
+      return;
+    }
+    st->alpha = ddiv(st->rho, sigma);
+  }
+};
+
+// S pass: s = r - alpha v ; t = A0 s ; (t,s), |t|^2, (rh,t), |s|^2 ; omega, rho, beta
+template <typename R>
+struct OpBsS {
+  static constexpr int NRED = 6;
+  static constexpr bool NEEDS_W = false;
+  BsBufs B;
+  long long N;
+  unsigned long long seed;
+  KState* st;
+  const cx<R>* r;
+  const cx<R>* v;
+  cx<R>* t;
+  cx<R> malpha;
+  __device__ bool skip() const { return ld_status(st) != ST_RUNNING; }
+  __device__ void prepare() {
+    const int k = __ldcg(&st->iter);
+    const int n = (k & 1) ^ 1;
+    r = (const cx<R>*)B.R[n];
+    v = (const cx<R>*)B.V[n];
+    t = (cx<R>*)B.T;
+    const dcx a = ld_dcx(&st->alpha);
+    malpha = mkc<R>((R)(-a.re), (R)(-a.im));
+  }
+  __device__ cx<R> load(int, long long idx) const { return caxpy(malpha, v[idx], r[idx]); }
+  __device__ void own(long long cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R>*,
+                      double* acc) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long idx = c * N + cell;
+      t[idx] = y[c];
+      acc_cdot<R>(acc, y[c], u[c]);                       // (t, s)
+      acc[2] += (double)cabs2(y[c]);                      // |t|^2
+      acc_cdot<R>(acc + 3, shadow<R>(idx, seed), y[c]);   // (rh, t)
+      acc[5] += (double)cabs2(u[c]);                      // |s|^2
+    }
+  }
+  __device__ void finish(const double* s) const {
+    const dcx ts = {s[0], s[1]};
+    const double tt = s[2];
+    const dcx rht = {s[3], s[4]};
+    const double ss = s[5];
+    st->iter += 1;
+    st->pending = 1;
+    if (!dfinite(ts) || !isfinite(tt) || !dfinite(rht) || !isfinite(ss)) {
+      st->status = ST_NONFINITE;
+      st->pending = 0;
+      return;
+    }
+    if (ss <= st->tol2 || tt <= 0.0) {
+      // s already small enough (or t vanished): finish with omega = 0
+      st->omega = {0.0, 0.0};
+      st->rr = ss;
+      check_progress(st, ss, true);
+      if (st->status == ST_RUNNING) st->status = ST_BREAKDOWN;
+      return;
+    }
+    const dcx om = {ts.re / tt, ts.im / tt};
+    st->omega = om;
+    double rr = ss - (ts.re * ts.re + ts.im * ts.im) / tt;
+    if (rr < 0.0) rr = 0.0;
+    st->rr = rr;
+    check_progress(st, rr, true);
+    if (st->status != ST_RUNNING) return;
+    const dcx rho_new = {-(om.re * rht.re - om.im * rht.im), -(om.re * rht.im + om.im * rht.re)};
+    if (dabs(om) <= 1e-300 || dabs(rho_new) <= 1e-300) {
+      st->status = ST_BREAKDOWN;
+      return;
+    }
+    // beta = (rho_new / rho) * (alpha / omega)
+    st->beta = dmul(ddiv(rho_new, st->rho), ddiv(st->alpha, om));
+    st->rho = rho_new;
+  }
+};
+
+// BiCGSTAB start: r = b - A0 x0 (x0 may be zero) ; rho = (rh, r) ; |r|^2 ; status.
+template <typename R>
+struct OpBsInit {
+  static constexpr int NRED = 3;
+  static constexpr bool NEEDS_W = false;
+  const cx<R>* b;
+  const cx<R>* x;
+  cx<R>* r;
+  long long N;
+  unsigned long long seed;
+  KState* st;
+  __device__ bool skip() const { return false; }
+  __device__ void prepare() {}
+  __device__ cx<R> load(int, long long idx) const { return x ? x[idx] : czero<R>(); }
+  __device__ void own(long long cell, int, int, int, const cx<R>*, const cx<R> y[3], const cx<R>*,
+                      double* acc) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long idx = c * N + cell;
+      const cx<R> rv = b[idx] - y[c];
+      r[idx] = rv;
+      acc_cdot<R>(acc, shadow<R>(idx, seed), rv);
+      acc[2] += (double)cabs2(rv);
+    }
+  }
+  __device__ void finish(const double* s) const {
+    st->rho = {s[0], s[1]};
+    st->rr = s[2];
+    st->iter = 0;
+    st->pending = 0;
+    st->status = ST_RUNNING;
+    check_progress(st, s[2], dfinite(st->rho));
+    if (st->status == ST_MAXITER) st->status = ST_RUNNING;
+  }
+};
+
+// Owed update after the loop stops: x += alpha p + omega (r - alpha v) on buffers
+// new = iter & 1 (the last P pass wrote r, v, p there).
+template <typename R>
+struct OpBsFinal {
+  static constexpr int NRED = 0;
+  static constexpr bool NEEDS_W = false;
+  BsBufs B;
+  long long N;
+  KState* st;
+  const cx<R>* r;
+  const cx<R>* v;
+  const cx<R>* p;
+  cx<R>* x;
+  cx<R> alpha, omega, malpha;
+  bool upd;
+  __device__ bool skip() const { return false; }
+  __device__ void prepare() {
+    const int k = __ldcg(&st->iter);
+    const int n = k & 1;
+    r = (const cx<R>*)B.R[n];
+    v = (const cx<R>*)B.V[n];
+    p = (const cx<R>*)B.P[n];
+    x = (cx<R>*)B.x;
+    upd = __ldcg(&st->pending) != 0;
+    alpha = from_d<R>(ld_dcx(&st->alpha));
+    omega = from_d<R>(ld_dcx(&st->omega));
+    malpha = mkc<R>(-alpha.re, -alpha.im);
+  }
+  __device__ void point(long long cell, int, int, int, const cx<R>*, double*) const {
+    if (!upd) return;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long idx = c * N + cell;
+      const cx<R> s = caxpy(malpha, v[idx], r[idx]);
+      x[idx] = caxpy(omega, s, caxpy(alpha, p[idx], x[idx]));
+    }
+  }
+  __device__ void finish(const double*) const {}
+};
+
+// ------------------------------------------------------------------ refinement (c128)
+// u = E_old + scale * d (d in the inner precision, optional) ; E_new = u ; r = b - A0 u ;
+// r32 = (complex64)(r * rscale) ; reduces |r|^2, sum|W||r|^2, sum|W|^2|r|^2,
+// (rh, r32) and |r32|^2 (the inner BiCGSTAB's starting rho and norm).
+template <typename RI>
+struct OpRefine {
+  static constexpr int NRED = 6;
+  static constexpr bool NEEDS_W = true;
+  const cx<double>* E_old;
+  const cx<RI>* d;
+  cx<double>* E_new;
+  const cx<double>* b;
+  cx<RI>* rin;
+  double scale, rscale;
+  long long N;
+  unsigned long long seed;
+  KState* st;
+  __device__ bool skip() const { return false; }
+  __device__ void prepare() {}
+  __device__ cx<double> load(int, long long idx) const {
+    cx<double> e = E_old[idx];
+    if (d) {
+      const cx<RI> dv = d[idx];
+      e = caxpy(mkc<double>(scale, 0.0), mkc<double>((double)dv.re, (double)dv.im), e);
+    }
+    return e;
+  }
+  __device__ void own(long long cell, int, int, int, const cx<double> u[3], const cx<double> y[3],
+                      const cx<double> W[3], double* acc) const {
+    double aW[3];
+    absW3<double>(W, aW);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long idx = c * N + cell;
+      E_new[idx] = u[c];
+      const cx<double> rv = b[idx] - y[c];
+      const cx<RI> r1 = mkc<RI>((RI)(rscale * rv.re), (RI)(rscale * rv.im));
+      rin[idx] = r1;
+      const double r2 = cabs2(rv);
+      acc[0] += r2;
+      acc[1] += aW[c] * r2;
+      acc[2] += aW[c] * aW[c] * r2;
+      acc_cdot<RI>(acc + 3, shadow<RI>(idx, seed), r1);
+      acc[5] += (double)cabs2(r1);
+    }
+  }
+  __device__ void finish(const double* s) const {
+    st->rr = s[0];
+    st->rr_pc = s[1];
+    st->rr_w2 = s[2];
+    st->extra[0] = s[3];
+    st->extra[1] = s[4];
+    st->extra[2] = s[5];
+  }
+};
+
+// FP64 residual of E for the unmasked right-hand side b0 = -i omega J:
+// r = b0 - A0 E (or b0 - A0^H E with `adjoint`, using A0^H = conj(W A0 W^-1 conj(.)));
+// reduces |r|^2, sum|W||r|^2 (forward) or sum|W|^-1|r|^2 (adjoint), |b0|^2 and the
+// matching weighted |b0|^2: the true and the symmetrised-system residuals.
+template <typename R>
+struct OpResidual {
+  static constexpr int NRED = 4;
+  static constexpr bool NEEDS_W = true;
+  const cx<R>* E;
+  const cx<R>* J;
+  double om_re, om_im;
+  int adjoint;
+  Geo<R> g;
+  double* out;  // 4 doubles
+  __device__ bool skip() const { return false; }
+  __device__ void prepare() {}
+  __device__ cx<R> w_at(int c, long long idx) const {
+    const long long cell = idx - c * g.N;
+    const long long YZ = (long long)g.Y * g.Z;
+    const int i = (int)(cell / YZ);
+    const int j = (int)((cell / g.Z) % g.Y);
+    const int k = (int)(cell % g.Z);
+    if (c == 0) return g.dxe[0][i] * g.dxh[1][j] * g.dxh[2][k];
+    if (c == 1) return g.dxh[0][i] * g.dxe[1][j] * g.dxh[2][k];
+    return g.dxh[0][i] * g.dxh[1][j] * g.dxe[2][k];
+  }
+  __device__ cx<R> load(int c, long long idx) const {
+    cx<R> e = E[idx];
+    if (adjoint) {
+      const cx<R> w = w_at(c, idx);
+      const R d = cabs2(w);
+      e = mkc<R>(w.re / d, -w.im / d) * cconj(e);
+    }
+    return e;
+  }
+  __device__ void own(long long cell, int, int, int, const cx<R>*, const cx<R> y[3], const cx<R> W[3],
+                      double* acc) const {
+    R aW[3];
+    absW3<R>(W, aW);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long idx = c * g.N + cell;
+      const cx<R> j = J[idx];
+      const cx<R> b0 = mkc<R>((R)(om_im * j.re + om_re * j.im), (R)(om_im * j.im - om_re * j.re));
+      const cx<R> ay = adjoint ? cconj(W[c] * y[c]) : y[c];
+      const cx<R> rv = b0 - ay;
+      const double wgt = adjoint ? 1.0 / (double)aW[c] : (double)aW[c];
+      acc[0] += (double)cabs2(rv);
+      acc[1] += wgt * (double)cabs2(rv);
+      acc[2] += (double)cabs2(b0);
+      acc[3] += wgt * (double)cabs2(b0);
+    }
+  }
+  __device__ void finish(const double* s) const {
+    out[0] = s[0];
+    out[1] = s[1];
+    out[2] = s[2];
+    out[3] = s[3];
+  }
+};
+
+// Copy / convert / zero helpers (pointwise over the 3 components of each cell).
+template <typename RS, typename RD>
+struct OpCopy {
+  static constexpr int NRED = 0;
+  static constexpr bool NEEDS_W = false;
+  const cx<RS>* src;  // null = zero fill
+  cx<RD>* dst;
+  long long N;
+  __device__ bool skip() const { return false; }
+  __device__ void prepare() {}
+  __device__ void point(long long cell, int, int, int, const void*, double*) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long idx = c * N + cell;
+      if (src) {
+        const cx<RS> v = src[idx];
+        dst[idx] = mkc<RD>((RD)v.re, (RD)v.im);
+      } else {
+        dst[idx] = mkc<RD>(RD(0), RD(0));
+      }
+    }
+  }
+  __device__ void finish(const double*) const {}
+};
+
+}  // namespace fdfd

@@ -1,0 +1,246 @@
+"""Device-resident FDFD wave operator (the plan behind every solve).
+
+``GridOperator`` uploads one problem definition -- ``omega``, ``dxes``,
+``epsilon`` and the optional ``mu`` / ``pec`` / ``pmc`` of the reference's
+``operators.e_full`` (``meanas/fdfd/operators.py:40-96``) -- builds a
+``libmeanas_fdfd`` plan over it and exposes the matrix-free products and the
+solver.  No sparse matrix is assembled: the plan holds 1D cell-width tables,
+``1/mu``, one mask byte per cell and (for mixed precision) complex64 copies.
+
+PyTorch is only the device-memory and stream carrier here; all arithmetic runs
+in the library's CUDA kernels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+from typing import Any
+
+import numpy
+import torch
+
+from . import _lib
+
+_OPS = {'A0': _lib.OP_A0, 'sym': _lib.OP_SYM, 'sym_h': _lib.OP_SYM_H}
+_PREC = {'c128': _lib.C128, 'c64': _lib.C64}
+_METHODS = {'cocg': _lib.METHOD_COCG, 'fp64': _lib.METHOD_COCG, 'mixed': _lib.METHOD_MIXED,
+            'bicgstab': _lib.METHOD_BICGSTAB}
+_CRITS = {'true': _lib.CRIT_TRUE, 'precond': _lib.CRIT_PRECOND, 'preconditioned': _lib.CRIT_PRECOND}
+
+
+@dataclasses.dataclass
+class SolveInfo:
+    """Outcome of one solve (the reference discards scipy's ``info``; this keeps it)."""
+    status: str
+    iterations: int
+    outer_iterations: int
+    residual: float        # ||b0 - A0 E|| / ||b0||  (FP64, recomputed on the result)
+    residual_pc: float     # residual of the symmetrised system generic() builds
+    kernel_launches: int
+    method: str
+    history: numpy.ndarray | None = None
+    kernel_ms: tuple = ()      # with profile=True: device ms of the iteration kernels by kind
+    kernel_count: tuple = ()   # (COCG stencil, COCG pointwise, BiCGSTAB P, BiCGSTAB S)
+
+    @property
+    def converged(self) -> bool:
+        return self.status == 'converged'
+
+
+def _device(device: Any | None) -> torch.device:
+    if device is None:
+        device = torch.device('cuda', torch.cuda.current_device())
+    device = torch.device(device)
+    if device.type != 'cuda':
+        raise ValueError('meanas_b200 runs on CUDA devices only')
+    return device
+
+
+def as_device(a: Any, dtype: torch.dtype, device: torch.device, n: int | None = None,
+              name: str = 'array') -> torch.Tensor:
+    """Contiguous device tensor of ``dtype`` (copies host arrays; converts device tensors)."""
+    if isinstance(a, torch.Tensor):
+        t = a.to(device=device, dtype=dtype)
+    else:
+        arr = numpy.asarray(a)
+        if dtype.is_complex:
+            arr = arr.astype(numpy.complex128 if dtype == torch.complex128 else numpy.complex64, copy=False)
+        else:
+            if numpy.iscomplexobj(arr):
+                raise ValueError(f'{name} must be real')
+            arr = arr.astype(numpy.float64, copy=False)
+        t = torch.from_numpy(numpy.ascontiguousarray(arr)).to(device=device, dtype=dtype)
+    t = t.reshape(-1).contiguous()
+    if n is not None and t.numel() != n:
+        raise ValueError(f'{name} has {t.numel()} elements, expected {n}')
+    return t
+
+
+def _stream_handle() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+class GridOperator:
+    """``A0 = pe (ch pm mu^-1 ce - omega^2 eps) pe`` on the device, with its solver."""
+
+    def __init__(self, omega: complex, dxes, epsilon, mu=None, pec=None, pmc=None, *,
+                 device: Any | None = None, fp32: bool = True):
+        self.lib = _lib.load()
+        self.device = _device(device)
+        self.omega = complex(omega)
+        self.shape = tuple(int(numpy.size(d)) for d in dxes[0])
+        if len(self.shape) != 3 or any(s < 1 for s in self.shape):
+            raise ValueError(f'bad grid shape {self.shape}')
+        if tuple(int(numpy.size(d)) for d in dxes[1]) != self.shape:
+            raise ValueError('dxes[0] and dxes[1] disagree on the grid shape')
+        self.n_cells = int(numpy.prod(self.shape))
+        self.n = 3 * self.n_cells
+        dev = self.device
+        with torch.cuda.device(dev):
+            self._keep: list[torch.Tensor] = []
+            dxe = [as_device(d, torch.complex128, dev, s, 'dx_e') for d, s in zip(dxes[0], self.shape)]
+            dxh = [as_device(d, torch.complex128, dev, s, 'dx_h') for d, s in zip(dxes[1], self.shape)]
+            # 1/dx as numpy computes it (the values the reference's sparse operators hold)
+            inv_e = [as_device(1 / numpy.asarray(d, dtype=complex), torch.complex128, dev) for d in dxes[0]]
+            inv_h = [as_device(1 / numpy.asarray(d, dtype=complex), torch.complex128, dev) for d in dxes[1]]
+            self.epsilon = as_device(epsilon, torch.float64, dev, self.n, 'epsilon')
+            self.mu = None if mu is None else as_device(mu, torch.float64, dev, self.n, 'mu')
+            self.pec = None if pec is None else as_device(pec, torch.float64, dev, self.n, 'pec')
+            self.pmc = None if pmc is None else as_device(pmc, torch.float64, dev, self.n, 'pmc')
+            self._keep += dxe + dxh + inv_e + inv_h
+            d = _lib.GridDesc()
+            d.shape[:] = self.shape
+            d.flags = _lib.GRID_FP32 if fp32 else 0
+            d.omega[:] = (self.omega.real, self.omega.imag)
+            for a in range(3):
+                d.dxe[a] = dxe[a].data_ptr()
+                d.dxh[a] = dxh[a].data_ptr()
+                d.inv_dxe[a] = inv_e[a].data_ptr()
+                d.inv_dxh[a] = inv_h[a].data_ptr()
+            d.epsilon = self.epsilon.data_ptr()
+            d.mu = self.mu.data_ptr() if self.mu is not None else None
+            d.pec = self.pec.data_ptr() if self.pec is not None else None
+            d.pmc = self.pmc.data_ptr() if self.pmc is not None else None
+            self._desc = d
+            nbytes = C.c_size_t()
+            _lib.check(self.lib.fdfd_plan_workspace_bytes(C.byref(d), C.byref(nbytes)))
+            self._plan_ws = torch.empty(max(int(nbytes.value), 256), dtype=torch.uint8, device=dev)
+            plan = C.c_void_p()
+            _lib.check(self.lib.fdfd_plan_create(C.byref(d), self._plan_ws.data_ptr(), nbytes.value,
+                                                 _stream_handle(), C.byref(plan)))
+            self._plan = plan
+            self.fp32 = fp32
+        self._solve_ws: dict[tuple, torch.Tensor] = {}
+
+    # ------------------------------------------------------------------ lifetime
+    def close(self) -> None:
+        if getattr(self, '_plan', None):
+            torch.cuda.synchronize(self.device)
+            self.lib.fdfd_plan_destroy(self._plan)
+            self._plan = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def plan(self) -> C.c_void_p:
+        if not self._plan:
+            raise RuntimeError('GridOperator is closed')
+        return self._plan
+
+    def set_xchunk(self, precision: str, xchunk: int) -> None:
+        """Override the x planes per CTA (autotuning hook); 0 restores the default."""
+        _lib.check(self.lib.fdfd_plan_set_xchunk(self.plan, _PREC[precision], int(xchunk)))
+
+    # ------------------------------------------------------------------ products
+    def apply(self, x, op: str = 'A0', precision: str = 'c128', out: torch.Tensor | None = None) -> torch.Tensor:
+        """``y = op(x)``: ``'A0'``, ``'sym'`` (Pl A0 Pr) or ``'sym_h'`` ((Pl A0 Pr)^H)."""
+        dt = torch.complex128 if precision == 'c128' else torch.complex64
+        xt = as_device(x, dt, self.device, self.n, 'x')
+        y = out if out is not None else torch.empty_like(xt)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.fdfd_apply(self.plan, _OPS[op], _PREC[precision], xt.data_ptr(),
+                                           y.data_ptr(), _stream_handle()))
+        return y
+
+    def residual(self, E, J) -> dict[str, float]:
+        """FP64 ``||b0 - A0 E||`` and ``||Pl (b0 - A0 E)||`` (absolute and relative)."""
+        Et = as_device(E, torch.complex128, self.device, self.n, 'E')
+        Jt = as_device(J, torch.complex128, self.device, self.n, 'J')
+        nbytes = C.c_size_t()
+        _lib.check(self.lib.fdfd_residual_workspace_bytes(self.plan, C.byref(nbytes)))
+        ws = torch.empty(int(nbytes.value), dtype=torch.uint8, device=self.device)
+        out = (C.c_double * 4)()
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.fdfd_residual(self.plan, Et.data_ptr(), Jt.data_ptr(), out, ws.data_ptr(),
+                                              nbytes.value, _stream_handle()))
+        r, rpc, b, bpc = list(out)
+        return dict(abs=r, rel=r / b if b else r, abs_pc=rpc, rel_pc=rpc / bpc if bpc else rpc, b=b, b_pc=bpc)
+
+    # ------------------------------------------------------------------ solve
+    def solve_opts(self, *, method: str = 'cocg', rtol: float = 1e-8, atol: float = 0.0,
+                   maxiter: int | None = None, criterion: str = 'true', adjoint: bool = False,
+                   chunk: int = 0, use_graph: bool = True, inner_rtol: float = 0.0, max_outer: int = 0,
+                   history: torch.Tensor | None = None, has_guess: bool = False,
+                   profile: bool = False) -> _lib.SolveOpts:
+        o = _lib.SolveOpts()
+        o.method = _METHODS[method]
+        o.criterion = _CRITS[criterion]
+        o.adjoint = int(bool(adjoint))
+        o.maxiter = int(maxiter if maxiter is not None else 10 * self.n)
+        o.maxiter = min(o.maxiter, 2 ** 31 - 1)
+        o.rtol = float(rtol)
+        o.atol = float(atol)
+        o.has_guess = int(bool(has_guess))
+        o.chunk = int(chunk)
+        o.use_graph = int(bool(use_graph))
+        o.max_outer = int(max_outer)
+        o.inner_rtol = float(inner_rtol)
+        o.history = history.data_ptr() if history is not None else None
+        o.profile = int(bool(profile))
+        return o
+
+    def workspace(self, opts: _lib.SolveOpts) -> torch.Tensor:
+        key = (opts.method,)
+        nbytes = C.c_size_t()
+        _lib.check(self.lib.fdfd_solve_workspace_bytes(self.plan, C.byref(opts), C.byref(nbytes)))
+        ws = self._solve_ws.get(key)
+        if ws is None or ws.numel() < nbytes.value:
+            ws = torch.empty(int(nbytes.value), dtype=torch.uint8, device=self.device)
+            self._solve_ws[key] = ws
+        return ws
+
+    def release_workspaces(self) -> None:
+        self._solve_ws.clear()
+
+    def solve(self, J, *, E_guess=None, out: torch.Tensor | None = None, record_history: bool = False,
+              **kw) -> tuple[torch.Tensor, SolveInfo]:
+        """Solve ``A0 E = -i omega J`` (or the adjoint) on the device; returns ``(E, info)``."""
+        Jt = as_device(J, torch.complex128, self.device, self.n, 'J')
+        E = out if out is not None else torch.empty(self.n, dtype=torch.complex128, device=self.device)
+        has_guess = E_guess is not None
+        if has_guess:
+            E.copy_(as_device(E_guess, torch.complex128, self.device, self.n, 'E_guess'))
+        hist = None
+        if record_history:
+            maxiter = kw.get('maxiter') or 10 * self.n
+            hist = torch.zeros(int(maxiter) + 1, dtype=torch.float64, device=self.device)
+        opts = self.solve_opts(history=hist, has_guess=has_guess, **kw)
+        ws = self.workspace(opts)
+        info = _lib.SolveInfo()
+        with torch.cuda.device(self.device):
+            rc = _lib.check(self.lib.fdfd_solve(self.plan, C.byref(opts), Jt.data_ptr(), E.data_ptr(),
+                                                ws.data_ptr(), ws.numel(), C.byref(info), _stream_handle()))
+        del rc
+        h = None
+        if hist is not None:
+            h = hist[:info.iterations + 1].cpu().numpy()
+        si = SolveInfo(status=_lib.STATUS_NAMES.get(info.status, str(info.status)), iterations=info.iterations,
+                       outer_iterations=info.outer_iterations, residual=info.residual,
+                       residual_pc=info.residual_pc, kernel_launches=info.kernel_launches,
+                       method=kw.get('method', 'cocg'), history=h,
+                       kernel_ms=tuple(info.kernel_ms), kernel_count=tuple(info.kernel_count))
+        return E, si

@@ -1,0 +1,231 @@
+"""CPU restatement (numpy / scipy) of the reference FDFD solve path.
+
+TEST INFRASTRUCTURE ONLY: this module is the parity checker and the timed CPU
+baseline.  The product path (``meanas_b200``) never imports it.
+
+Parity pinning: ``tests/golden/make_golden.py`` runs the reference itself
+(``meanas.fdfd.operators.e_full``, ``e_full_preconditioners``,
+``solvers.generic`` and ``scpml``) on small grids and stores inputs/outputs as
+``tests/golden/*.npz``; ``tests/test_oracle.py`` checks every function below
+against those vectors.
+
+What each function restates:
+
+* ``e_full_apply``   matrix-free ``A0 @ E`` with the semantics of the sparse
+  ``meanas/fdfd/operators.py:40-96``: ``pe (ch pm diag(1/mu) ce - omega^2 diag(eps)) pe``,
+  using the periodic ``roll`` derivatives of ``meanas/fdmath/functional.py:16-122``.
+  (Note the sparse form divides by ``mu``; the functional
+  ``meanas/fdfd/functional.py:45`` multiplies.  ``generic()`` uses the sparse form,
+  so this follows it.)
+* ``e_full_csr``     the same operator assembled as CSR in complex128, built from
+  periodic shift matrices like ``meanas/fdmath/operators.py:15-52,99-171,222-251``.
+* ``precond_p2``     ``p^2`` of ``meanas/fdfd/operators.py:116-118`` (per component
+  products of 1D widths); ``Pl = sqrt(p^2)``, ``Pr = 1/Pl`` (``:120-122``).
+* ``generic_qmr``    ``meanas/fdfd/solvers.py:66-141`` with the default
+  ``_scipy_qmr`` (``:21-63``): the symmetrised CSR system handed to
+  ``scipy.sparse.linalg.qmr``.  QMR itself is third-party (scipy; the reference
+  pins ``scipy~=1.14`` in ``pyproject.toml:44``, ``uv.lock`` locks 1.16.3); it
+  is called, not restated.  The adjoint branch (``:119-137``) is written with
+  explicit conjugate transposes, since ``csr_array.H`` is gone in SciPy >= 1.14.
+* ``cocg``           complex-symmetric CG in the E-space with the ``p^2``-weighted
+  bilinear form: algebraically the COCG iteration on ``Pl A0 Pr`` (the system
+  ``generic()`` builds) rewritten with ``x = Pl E``; the GPU solver runs the same
+  recurrence.
+"""
+from __future__ import annotations
+
+import numpy
+from numpy.typing import NDArray
+from scipy import sparse
+import scipy.sparse.linalg
+
+
+def _shape_of(dxes) -> tuple[int, int, int]:
+    return tuple(int(numpy.size(d)) for d in dxes[0])
+
+
+def _bcast(a: NDArray, axis: int) -> NDArray:
+    idx = [None, None, None]
+    idx[axis] = slice(None)
+    return numpy.asarray(a)[tuple(idx)]
+
+
+def _dfwd(f: NDArray, dx: NDArray, axis: int) -> NDArray:
+    return (numpy.roll(f, -1, axis=axis) - f) / _bcast(dx, axis)
+
+
+def _dback(f: NDArray, dx: NDArray, axis: int) -> NDArray:
+    return (f - numpy.roll(f, 1, axis=axis)) / _bcast(dx, axis)
+
+
+def curl_forward(dx_e, e: NDArray) -> NDArray:
+    """Forward curl of a (3,X,Y,Z) field, ``meanas/fdmath/functional.py:67-91``."""
+    out = numpy.empty_like(e)
+    out[0] = _dfwd(e[2], dx_e[1], 1) - _dfwd(e[1], dx_e[2], 2)
+    out[1] = _dfwd(e[0], dx_e[2], 2) - _dfwd(e[2], dx_e[0], 0)
+    out[2] = _dfwd(e[1], dx_e[0], 0) - _dfwd(e[0], dx_e[1], 1)
+    return out
+
+
+def curl_back(dx_h, h: NDArray) -> NDArray:
+    """Backward curl of a (3,X,Y,Z) field, ``meanas/fdmath/functional.py:94-122``."""
+    out = numpy.empty_like(h)
+    out[0] = _dback(h[2], dx_h[1], 1) - _dback(h[1], dx_h[2], 2)
+    out[1] = _dback(h[0], dx_h[2], 2) - _dback(h[2], dx_h[0], 0)
+    out[2] = _dback(h[1], dx_h[0], 0) - _dback(h[0], dx_h[1], 1)
+    return out
+
+
+def e_full_apply(omega, dxes, epsilon, E, mu=None, pec=None, pmc=None) -> NDArray:
+    """``A0 @ E`` for 1D C-order vectors (length 3XYZ); returns complex128 (3XYZ,)."""
+    shape = _shape_of(dxes)
+    f3 = (3, *shape)
+    e = numpy.asarray(E, dtype=complex).reshape(f3)
+    eps = numpy.asarray(epsilon).reshape(f3)
+    if pec is not None:
+        e = e * numpy.where(numpy.asarray(pec).reshape(f3), 0, 1)
+    h = curl_forward(dxes[0], e)
+    if mu is not None:
+        h = h / numpy.asarray(mu).reshape(f3)
+    if pmc is not None:
+        h = h * numpy.where(numpy.asarray(pmc).reshape(f3), 0, 1)
+    y = curl_back(dxes[1], h) - omega ** 2 * eps * e
+    if pec is not None:
+        y = y * numpy.where(numpy.asarray(pec).reshape(f3), 0, 1)
+    return y.ravel()
+
+
+def precond_p2(dxes) -> NDArray:
+    """(3,X,Y,Z) complex ``p^2``: x: dxe_x dxh_y dxh_z, y: dxh_x dxe_y dxh_z, z: dxh_x dxh_y dxe_z."""
+    (ex, ey, ez), (hx, hy, hz) = dxes
+    ex, ey, ez, hx, hy, hz = (numpy.asarray(v, dtype=complex) for v in (ex, ey, ez, hx, hy, hz))
+    return numpy.stack([
+        ex[:, None, None] * hy[None, :, None] * hz[None, None, :],
+        hx[:, None, None] * ey[None, :, None] * hz[None, None, :],
+        hx[:, None, None] * hy[None, :, None] * ez[None, None, :],
+    ])
+
+
+def precond_pl(dxes) -> NDArray:
+    """1D ``Pl`` diagonal: principal-branch ``sqrt(p^2)`` (``Pr = 1/Pl``)."""
+    return numpy.sqrt(precond_p2(dxes).ravel())
+
+
+def _shift_matrix(shape, axis: int) -> sparse.csr_array:
+    """``(S f)[..i..] = f[..(i+1) mod n..]`` along ``axis``."""
+    n = int(numpy.prod(shape))
+    idx = numpy.arange(n).reshape(shape)
+    cols = numpy.roll(idx, -1, axis=axis).ravel()
+    return sparse.csr_array((numpy.ones(n), (numpy.arange(n), cols)), shape=(n, n))
+
+
+def _cell_widths(dx1d, shape, axis) -> NDArray:
+    return numpy.broadcast_to(_bcast(numpy.asarray(dx1d), axis), shape).ravel()
+
+
+def e_full_csr(omega, dxes, epsilon, mu=None, pec=None, pmc=None) -> sparse.csr_array:
+    """CSR ``A0`` (complex128, 3XYZ x 3XYZ)."""
+    shape = _shape_of(dxes)
+    n = int(numpy.prod(shape))
+    eye = sparse.eye_array(n, format='csr')
+    Df, Db = [], []
+    for a in range(3):
+        S = _shift_matrix(shape, a)
+        Df.append(sparse.diags_array(1 / _cell_widths(dxes[0][a], shape, a)) @ (S - eye))
+        Db.append(sparse.diags_array(1 / _cell_widths(dxes[1][a], shape, a)) @ (eye - S.T))
+
+    def cross(D):
+        z = sparse.csr_array((n, n))
+        return sparse.block_array([[z, -D[2], D[1]], [D[2], z, -D[0]], [-D[1], D[0], z]])
+    ce = cross(Df)
+    ch = cross(Db)
+    N3 = 3 * n
+    pe = sparse.diags_array(numpy.where(pec, 0.0, 1.0) if pec is not None else numpy.ones(N3))
+    pm = sparse.diags_array(numpy.where(pmc, 0.0, 1.0) if pmc is not None else numpy.ones(N3))
+    md = sparse.diags_array(1 / numpy.asarray(mu) if mu is not None else numpy.ones(N3))
+    ed = sparse.diags_array(numpy.asarray(epsilon))
+    return (pe @ (ch @ pm @ md @ ce - omega ** 2 * ed) @ pe).tocsr()
+
+
+def true_residual(omega, dxes, epsilon, E, J, mu=None, pec=None, pmc=None) -> float:
+    """``||A0 E - b0|| / ||b0||`` with ``b0 = -i omega J`` (``meanas/test/test_fdfd.py:15-18``)."""
+    b0 = -1j * omega * numpy.asarray(J)
+    r = e_full_apply(omega, dxes, epsilon, E, mu, pec, pmc) - b0
+    return float(numpy.linalg.norm(r) / numpy.linalg.norm(b0))
+
+
+def generic_qmr(omega, dxes, J, epsilon, mu=None, *, pec=None, pmc=None, adjoint=False,
+                rtol=1e-8, atol=0.0, maxiter=None, E_guess=None, counter=None):
+    """Reference ``generic()`` + ``_scipy_qmr`` on the CPU: assemble, symmetrise, scipy QMR."""
+    b0 = -1j * omega * numpy.asarray(J)
+    A0 = e_full_csr(omega, dxes, epsilon, mu, pec, pmc)
+    pl = precond_pl(dxes)
+    Pl = sparse.diags_array(pl)
+    Pr = sparse.diags_array(1 / pl)
+    if adjoint:
+        A = (Pl @ A0 @ Pr).conj().T
+        b = Pr.conj().T @ b0
+    else:
+        A = Pl @ A0 @ Pr
+        b = Pl @ b0
+    kw = dict(rtol=rtol, atol=atol)
+    if maxiter is not None:
+        kw['maxiter'] = maxiter
+    if E_guess is not None:
+        kw['x0'] = (Pr.conj().T if adjoint else Pl) @ numpy.asarray(E_guess)
+    if counter is not None:
+        def cb(_xk):
+            counter[0] += 1
+        kw['callback'] = cb
+    x, info = scipy.sparse.linalg.qmr(A.tocsr(), b, **kw)
+    E = (Pl.conj().T @ x) if adjoint else (Pr @ x)
+    return E, info
+
+
+BREAKDOWN_RATIO = 1e-14
+
+
+def cocg(omega, dxes, epsilon, b0, mu=None, pec=None, pmc=None, *, rtol=1e-8, maxiter=100000,
+         x0=None, history=None):
+    """E-space COCG: solves ``A0 E = b0`` with bilinear form ``<u, v> = sum(u * p^2 * v)``.
+
+    Stops when the true residual ``||b0 - A0 E||`` (recurrence value) is
+    ``<= rtol ||b0||``.  Returns ``(E, iterations, status)`` with status 0 =
+    converged, 1 = maxiter, 2 = breakdown.
+    """
+    W = precond_p2(dxes).ravel()
+    mask = numpy.where(pec, 0, 1) if pec is not None else None
+    b0 = numpy.asarray(b0, dtype=complex)
+    if mask is not None:
+        b0 = b0 * mask
+
+    def A(v):
+        return e_full_apply(omega, dxes, epsilon, v, mu, pec, pmc)
+    x = numpy.zeros_like(b0) if x0 is None else numpy.array(x0, dtype=complex)
+    r = b0 - A(x) if x0 is not None else b0.copy()
+    p = numpy.zeros_like(b0)
+    bnorm = numpy.linalg.norm(b0)
+    aW = numpy.abs(W)
+    rho = numpy.sum(r * W * r)
+    beta = 0.0
+    for it in range(maxiter):
+        if numpy.linalg.norm(r) <= rtol * bnorm:
+            return x, it, 0
+        # (near) breakdown: the unconjugated form cancelled below 1e-14 of its bound
+        if abs(rho) <= BREAKDOWN_RATIO * numpy.sum(aW * abs(r) ** 2):
+            return x, it, 2
+        p = r + beta * p
+        q = A(p)
+        sigma = numpy.sum(p * W * q)
+        bound = numpy.sqrt(numpy.sum(aW * abs(p) ** 2) * numpy.sum(aW * abs(q) ** 2))
+        if not numpy.isfinite(sigma) or abs(sigma) <= BREAKDOWN_RATIO * bound:
+            return x, it, 2
+        alpha = rho / sigma
+        x = x + alpha * p
+        r = r - alpha * q
+        rho_new = numpy.sum(r * W * r)
+        beta = rho_new / rho
+        rho = rho_new
+        if history is not None:
+            history.append(numpy.linalg.norm(r) / bnorm)
+    return x, maxiter, 1

@@ -1,0 +1,265 @@
+"""Generate tests/golden/*.npz by running the reference meanas itself.
+
+Run from the repository root, where the reference checkout is mounted:
+
+    python tests/golden/make_golden.py /root/reference
+
+The reference is pure Python (numpy/scipy) and imports directly; this script is
+the only place that reads it.  Outputs:
+
+* ``scpml.npz``     ``stretch_with_scpml`` / ``uniform_grid_scpml`` cell widths.
+* ``operator.npz``  random small problems (PML, non-uniform widths, eps, mu, PEC,
+                    PMC) with ``e_full @ x``, ``(Pl e_full Pr) @ x``, its conjugate
+                    transpose applied to x, and ``Pl``.
+* ``solve.npz``     reference ``generic()`` solutions: the grids and fixtures of
+                    ``meanas/test/test_fdfd.py`` / ``conftest.py`` (rtol 1e-11,
+                    atol 1e-15), the 1D PML cases of ``meanas/test/test_fdfd_pml.py``
+                    (their unidirectional sources included), and 3D PML problems
+                    with mu, PEC and PMC, forward and adjoint.
+* ``dipole48.npz``  reference ``generic()`` on the 48^3 dipole-in-core problem
+                    (rtol 1e-8, scipy QMR): field stored as complex64.
+"""
+from __future__ import annotations
+
+import sys
+import time
+from pathlib import Path
+
+import numpy
+
+REF = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+sys.path.insert(0, REF)
+sys.path.insert(0, str(Path(__file__).resolve().parents[2]))
+
+import scipy.sparse  # noqa: E402
+from meanas.fdfd import operators, scpml, solvers, waveguide_3d  # noqa: E402
+from meanas.fdmath import vec, unvec  # noqa: E402
+
+# generic(adjoint=True) uses csr_array.H, which SciPy >= 1.14 removed.
+if not hasattr(scipy.sparse.csr_array, 'H'):
+    scipy.sparse.csr_array.H = property(lambda s: s.conj().T)
+    scipy.sparse.dia_array.H = property(lambda s: s.conj().T)
+
+OUT = Path(__file__).resolve().parent
+
+
+def pack_dxes(prefix: str, dxes, out: dict) -> None:
+    for g in range(2):
+        for a in range(3):
+            out[f'{prefix}dx{g}{a}'] = numpy.asarray(dxes[g][a], dtype=complex)
+
+
+def gen_scpml() -> None:
+    out = {}
+    cases = [((48, 48, 48), 2 * numpy.pi / 30, 10, 1.0, -16, 3.5),
+             ((20, 17, 9), 0.7, 4, 1.3, -12, 4.0),
+             ((30, 1, 1), 1 / 1500, 10, 2.5, -16, 4.0),
+             ((64, 40, 33), 2 * numpy.pi / 26, 7, 2.1, -20, 3.0)]
+    for n, (shape, om, th, eff, lnr, m) in enumerate(cases):
+        dxes = [[numpy.ones(s) for s in shape] for _ in range(2)]
+        sf = scpml.prepare_s_function(ln_R=lnr, m=m)
+        for ax in range(3):
+            if shape[ax] <= 2 * th:
+                continue
+            for pol in (-1, 1):
+                dxes = scpml.stretch_with_scpml(dxes, axis=ax, polarity=pol, omega=om,
+                                                epsilon_effective=eff, thickness=th, s_function=sf)
+        out[f'c{n}_params'] = numpy.array([om, th, eff, lnr, m])
+        out[f'c{n}_shape'] = numpy.array(shape)
+        pack_dxes(f'c{n}_', dxes, out)
+        u = scpml.uniform_grid_scpml(shape, [min(th, s // 3) for s in shape], om, eff)
+        pack_dxes(f'c{n}_u', u, out)
+        out[f'c{n}_uth'] = numpy.array([min(th, s // 3) for s in shape])
+    out['n'] = numpy.array(len(cases))
+    numpy.savez_compressed(OUT / 'scpml.npz', **out)
+
+
+def gen_operator() -> None:
+    rng = numpy.random.default_rng(2024)
+    out = {}
+    cases = [((6, 5, 4), True, True, True, 2),
+             ((7, 6, 1), False, True, False, 2),
+             ((1, 6, 7), True, False, True, 0),
+             ((9, 8, 7), False, False, False, 3),
+             ((12, 10, 8), True, True, True, 3),
+             ((5, 1, 5), False, False, False, 0),
+             ((21, 9, 34), True, True, True, 4),
+             ((4, 37, 1), True, True, True, 1)]
+    for n, (shape, use_mu, use_pec, use_pmc, th) in enumerate(cases):
+        om = complex(2 * numpy.pi / rng.uniform(6, 12), 0.0) if n != 3 else complex(0.9, 0.05)
+        dxes = [[rng.uniform(0.8, 1.3, s) for s in shape] for _ in range(2)]
+        sf = scpml.prepare_s_function(ln_R=-16, m=3.5)
+        for ax in range(3):
+            if shape[ax] > 2 * th + 1 and th > 0:
+                for pol in (-1, 1):
+                    dxes = scpml.stretch_with_scpml(dxes, axis=ax, polarity=pol, omega=om.real,
+                                                    thickness=th, s_function=sf)
+        N3 = 3 * int(numpy.prod(shape))
+        eps = rng.uniform(1, 12.1, N3)
+        mu = rng.uniform(1, 1.5, N3) if use_mu else None
+        pec = (rng.random(N3) < 0.08).astype(float) if use_pec else None
+        pmc = (rng.random(N3) < 0.05).astype(float) if use_pmc else None
+        x = rng.standard_normal(N3) + 1j * rng.standard_normal(N3)
+        A0 = operators.e_full(om, dxes, eps, mu, pec, pmc).tocsr()
+        Pl, Pr = operators.e_full_preconditioners(dxes)
+        S = (Pl @ A0 @ Pr).tocsr()
+        p = f'c{n}_'
+        out[p + 'shape'] = numpy.array(shape)
+        out[p + 'omega'] = numpy.array(om)
+        pack_dxes(p, dxes, out)
+        out[p + 'eps'] = eps
+        for name, arr in (('mu', mu), ('pec', pec), ('pmc', pmc)):
+            if arr is not None:
+                out[p + name] = arr
+        out[p + 'x'] = x
+        out[p + 'A0x'] = A0 @ x
+        out[p + 'Sx'] = S @ x
+        out[p + 'SHx'] = S.conj().T @ x
+        out[p + 'pl'] = Pl.diagonal()
+    out['n'] = numpy.array(len(cases))
+    numpy.savez_compressed(OUT / 'operator.npz', **out)
+
+
+def gen_solve() -> None:
+    """Reference generic() solutions."""
+    rng = numpy.random.RandomState(12345)
+    out = {}
+    n = 0
+    om = 1 / 1500
+
+    def store(tag, shape, dxes, eps, J, E, om, mu=None, pec=None, pmc=None, adjoint=False, extra=None):
+        nonlocal n
+        p = f'c{n}_'
+        out[p + 'tag'] = numpy.array(tag)
+        out[p + 'shape'] = numpy.array(shape)
+        out[p + 'omega'] = numpy.array(complex(om))
+        pack_dxes(p, dxes, out)
+        out[p + 'eps'] = eps
+        out[p + 'J'] = J
+        out[p + 'E'] = E
+        out[p + 'adjoint'] = numpy.array(adjoint)
+        for name, arr in (('mu', mu), ('pec', pec), ('pmc', pmc)):
+            if arr is not None:
+                out[p + name] = arr
+        for k, v in (extra or {}).items():
+            out[p + k] = v
+        n += 1
+
+    # meanas/test/test_fdfd.py fixtures (test_residual / test_poynting_planes)
+    for shape in [(5, 5, 1), (5, 1, 5), (5, 5, 5)]:
+        is3d = 1 not in shape
+        for eps_kind in ['center', '000', 'random']:
+            for bg in [1.0, 1.5]:
+                for fg in [1.0, 2.5]:
+                    if is3d and (eps_kind == '000' or bg != 1 or fg not in (1.0, 2.0)):
+                        continue
+                    for dxk in ['uniform', 'centerbig']:
+                        for dx in [1.0, 1.5]:
+                            eps = numpy.full((3, *shape), bg)
+                            if eps_kind == 'center':
+                                eps[:, shape[0] // 2, shape[1] // 2, shape[2] // 2] = fg
+                            elif eps_kind == '000':
+                                eps[:, 0, 0, 0] = fg
+                            else:
+                                eps[:] = rng.uniform(low=min(bg, fg), high=max(bg, fg), size=(3, *shape))
+                            dxes = [[numpy.full(s, dx) for s in shape] for _ in range(2)]
+                            if dxk == 'centerbig':
+                                for eh in (0, 1):
+                                    for ax in (0, 1, 2):
+                                        dxes[eh][ax][dxes[eh][ax].size // 2] *= 1.1
+                            j = numpy.zeros((3, *shape), dtype=complex)
+                            cm = numpy.zeros((3, *shape), dtype=bool)
+                            cm[:, shape[0] // 2, shape[1] // 2, shape[2] // 2] = True
+                            j[numpy.roll(cm, [1, 1, 1], axis=(1, 2, 3))] = 1 + 1j
+                            j[numpy.roll(cm, [-1, -1, -1], axis=(1, 2, 3))] = 1 - 1j
+                            E = solvers.generic(J=vec(j), omega=om, dxes=dxes, epsilon=vec(eps),
+                                                matrix_solver_opts=dict(atol=1e-15, rtol=1e-11))
+                            store('test_fdfd', shape, dxes, vec(eps), vec(j), E, om)
+
+    # meanas/test/test_fdfd_pml.py (test_pml): 1D grids, PML on the propagation axis
+    for shape in [(30, 1, 1), (1, 30, 1), (1, 1, 30)]:
+        for pol in (+1, -1):
+            for fg in (1.0, 2.5):
+                for dx in (1.0, 1.5):
+                    sh3 = (3, *shape)
+                    eps = numpy.full(sh3, fg)
+                    dxes = [[numpy.full(s, dx) for s in shape] for _ in range(2)]
+                    dim = numpy.where(numpy.array(shape) > 1)[0][0]
+                    for p_ in (-1, 1):
+                        dxes = scpml.stretch_with_scpml(dxes, axis=dim, polarity=p_, omega=om,
+                                                        epsilon_effective=fg, thickness=10)
+                    other = [0, 1, 2]
+                    other.remove(dim)
+                    dx_prop = (dxes[0][dim][shape[dim] // 2] + dxes[1][dim][shape[dim] // 2]) / 2
+                    cm = numpy.zeros(sh3, dtype=bool)
+                    cm[other, shape[0] // 2, shape[1] // 2, shape[2] // 2] = True
+                    k = om * numpy.sqrt(eps[cm].mean())
+                    kc = 2 / dx_prop * numpy.arcsin(k * dx_prop / 2)
+                    e = numpy.zeros_like(eps, dtype=complex)
+                    e[cm] = 1 / numpy.linalg.norm(cm[:])
+                    sl = [slice(None)] * 3
+                    sl[dim] = slice(shape[dim] // 2, shape[dim] // 2 + 1)
+                    j = waveguide_3d.compute_source(E=e, wavenumber=kc, omega=om, dxes=dxes, axis=dim,
+                                                    polarity=pol, slices=sl, epsilon=eps)
+                    E = solvers.generic(J=vec(j), omega=om, dxes=dxes, epsilon=vec(eps),
+                                        matrix_solver_opts={'atol': 1e-15, 'rtol': 1e-11})
+                    store('test_pml', shape, [list(d) for d in dxes], vec(eps), vec(j), E, om,
+                          extra=dict(src_polarity=numpy.array(pol)))
+
+    # 3D PML problems with mu / PEC / PMC, forward and adjoint
+    r2 = numpy.random.default_rng(7)
+    for shape, th, use_mu, use_masks in [((12, 10, 8), 3, True, True), ((10, 9, 7), 2, False, True),
+                                         ((14, 12, 1), 3, True, False), ((11, 8, 9), 2, True, True)]:
+        om2 = 2 * numpy.pi / 8
+        dxes = [[r2.uniform(0.9, 1.1, s) for s in shape] for _ in range(2)]
+        for ax in range(3):
+            if shape[ax] > 2 * th + 1:
+                for p_ in (-1, 1):
+                    dxes = scpml.stretch_with_scpml(dxes, axis=ax, polarity=p_, omega=om2, thickness=th)
+        N3 = 3 * int(numpy.prod(shape))
+        eps = r2.uniform(1, 12, N3)
+        mu = r2.uniform(1, 1.5, N3) if use_mu else None
+        pec = (r2.random(N3) < 0.05).astype(float) if use_masks else None
+        pmc = (r2.random(N3) < 0.03).astype(float) if use_masks else None
+        J = numpy.zeros((3, *shape), dtype=complex)
+        c = tuple(s // 2 for s in shape)
+        J[(2, *c)] = 1.0
+        J[(0, *c)] = 0.5j
+        Jv = vec(J)
+        if pec is not None:
+            Jv = Jv * (pec == 0)
+        for adjoint in (False, True):
+            E = solvers.generic(omega=om2, dxes=dxes, J=Jv, epsilon=eps, mu=mu, pec=pec, pmc=pmc,
+                                adjoint=adjoint, matrix_solver_opts=dict(rtol=1e-12, atol=0))
+            store('pml3d', shape, dxes, eps, Jv, E, om2, mu, pec, pmc, adjoint=adjoint)
+    out['n'] = numpy.array(n)
+    numpy.savez_compressed(OUT / 'solve.npz', **out)
+
+
+def gen_dipole48() -> None:
+    from meanas_b200 import workloads
+    p = workloads.dipole_core(48)
+    it = [0]
+
+    def qmr_counting(A, b, **kw):
+        def cb(_):
+            it[0] += 1
+        return scipy.sparse.linalg.qmr(A, b, callback=cb, **kw)[0]
+    t0 = time.perf_counter()
+    E = solvers.generic(p.omega, p.dxes, p.J, p.epsilon, matrix_solver=qmr_counting,
+                        matrix_solver_opts=dict(rtol=1e-8, atol=0))
+    t1 = time.perf_counter()
+    A0 = operators.e_full(p.omega, p.dxes, p.epsilon).tocsr()
+    b0 = -1j * p.omega * p.J
+    res = numpy.linalg.norm(A0 @ E - b0) / numpy.linalg.norm(b0)
+    numpy.savez_compressed(OUT / 'dipole48.npz', E=E.astype(numpy.complex64), qmr_iterations=it[0],
+                           seconds=t1 - t0, residual=res)
+    print('dipole48', it[0], t1 - t0, res)
+
+
+if __name__ == '__main__':
+    which = sys.argv[2:] or ['scpml', 'operator', 'solve', 'dipole48']
+    for w in which:
+        t = time.perf_counter()
+        globals()[f'gen_{w}']()
+        print(w, f'{time.perf_counter() - t:.1f}s')

@@ -1,0 +1,80 @@
+"""The C-ABI library: it loads without a GPU, exports every declared entry point,
+and its ctypes mirror matches the C structures byte for byte."""
+from __future__ import annotations
+
+import re
+import shutil
+import subprocess
+from pathlib import Path
+
+import ctypes as C
+import pytest
+
+from conftest import ROOT
+
+HEADER = ROOT / 'include' / 'meanas_fdfd.h'
+
+
+def declared_functions() -> list[str]:
+    text = HEADER.read_text()
+    text = re.sub(r'/\*.*?\*/', '', text, flags=re.S)
+    return sorted(set(re.findall(r'\b(fdfd_[a-z0-9_]+)\s*\(', text)))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    from meanas_b200 import _lib
+    lib = _lib.load()
+    names = declared_functions()
+    assert names, 'no declarations found'
+    for name in names:
+        assert hasattr(lib, name), name
+    assert set(names) == set(_lib.EXPORTS), set(names) ^ set(_lib.EXPORTS)
+    assert lib.fdfd_abi_version() == _lib.ABI_VERSION
+
+
+def test_struct_layouts_match_header(tmp_path: Path):
+    from meanas_b200 import _lib
+    cc = shutil.which('gcc') or shutil.which('cc')
+    if cc is None:
+        pytest.skip('no C compiler')
+    src = tmp_path / 'sz.c'
+    src.write_text(f'''#include <stdio.h>
+#include <stddef.h>
+#include "{HEADER}"
+int main(void) {{
+  printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(fdfd_grid_desc), sizeof(fdfd_solve_opts),
+         sizeof(fdfd_solve_info), offsetof(fdfd_grid_desc, epsilon), offsetof(fdfd_solve_opts, history),
+         offsetof(fdfd_solve_info, residual));
+  return 0;
+}}
+''')
+    exe = tmp_path / 'sz'
+    subprocess.run([cc, str(src), '-o', str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = [C.sizeof(_lib.GridDesc), C.sizeof(_lib.SolveOpts), C.sizeof(_lib.SolveInfo),
+            _lib.GridDesc.epsilon.offset, _lib.SolveOpts.history.offset, _lib.SolveInfo.residual.offset]
+    assert got == want
+
+
+def test_argument_errors_need_no_gpu():
+    """Calls that fail argument checks return negative codes and a message."""
+    from meanas_b200 import _lib
+    lib = _lib.load()
+    d = _lib.GridDesc()
+    d.shape[:] = (0, 4, 4)
+    nbytes = C.c_size_t()
+    rc = lib.fdfd_plan_workspace_bytes(C.byref(d), C.byref(nbytes))
+    assert rc == -1
+    assert b'shape' in lib.fdfd_last_error()
+    d.shape[:] = (4, 5, 6)
+    d.mu = 1  # any non-NULL pointer: only the layout is computed
+    assert lib.fdfd_plan_workspace_bytes(C.byref(d), C.byref(nbytes)) == 0
+    assert nbytes.value > 3 * 120 * 8
+    assert lib.fdfd_plan_destroy(None) == 0
+
+
+def test_no_cpu_fallback_in_product_package():
+    """The product package never imports the oracle."""
+    for p in (ROOT / 'meanas_b200').rglob('*.py'):
+        text = p.read_text()
+        assert 'from oracle' not in text and 'import oracle' not in text, p
