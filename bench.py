@@ -199,7 +199,7 @@ def run_ours(args) -> dict | None:
 
     out = {}
     with Clocks(local) as clk:
-        for method in ('mixed', 'cocg'):
+        for method in args.methods.split(','):
             total_ms, lats, infos = timed(method, args.steps, args.warmup, profile=True)
             assert all(i.converged and i.residual <= RTOL for i in infos), infos
             kms = numpy.sum([i.kernel_ms for i in infos], axis=0)
@@ -258,9 +258,12 @@ def run_ours(args) -> dict | None:
         'data': 'synthetic (seeded)',
         'config': dict(WORKLOAD, method=best, parallelism=f'replicas x{world}'),
         'p50_ms': round(b['p50_ms'], 3), 'p99_ms': round(b['p99_ms'], 3),
-        'mixed': {k: v for k, v in out['mixed'].items() if k not in ('kernel_ms', 'kernel_count')},
-        'fp64': {k: v for k, v in out['cocg'].items() if k not in ('kernel_ms', 'kernel_count')},
-        'mixed_over_fp64': round(out['mixed']['solves_per_s'] / out['cocg']['solves_per_s'], 3),
+        'mixed': ({k: v for k, v in out['mixed'].items() if k not in ('kernel_ms', 'kernel_count')}
+                  if 'mixed' in out else None),
+        'fp64': ({k: v for k, v in out['cocg'].items() if k not in ('kernel_ms', 'kernel_count')}
+                 if 'cocg' in out else None),
+        'mixed_over_fp64': (round(out['mixed']['solves_per_s'] / out['cocg']['solves_per_s'], 3)
+                            if 'mixed' in out and 'cocg' in out else None),
         'roofline': {'bound': 'hbm', 'kernel': KERNEL_NAMES[dom], 'achieved': round(achieved, 1),
                      'peak': peak, 'unit': 'GB/s', 'frac': round(achieved / peak, 4),
                      'peak_kind': peak_kind, 'traffic': traffic,
@@ -271,8 +274,8 @@ def run_ours(args) -> dict | None:
         'e2e': e2e,
     }
     if world == 1 and args.cpu_sample_iters > 0:
-        res['cpu_baseline'] = cpu_baseline(p, args.cpu_sample_iters, b['iterations'] if best == 'cocg'
-                                           else out['cocg']['iterations'])
+        res['cpu_baseline'] = cpu_baseline(p, args.cpu_sample_iters,
+                                           out['cocg']['iterations'] if 'cocg' in out else b['iterations'])
     return res
 
 
@@ -321,17 +324,60 @@ def run_reference(args) -> dict | None:
             'e2e': {'value': v, 'unit': 'solves/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
 
 
+def kernel_mode(args) -> None:
+    """A few iterations of each solver on one problem (for ncu captures): COCG (complex128),
+    the mixed solver (complex64 BiCGSTAB passes + complex128 refinement) and the
+    matrix-free products; prints per-kernel event timings."""
+    import torch
+    from meanas_b200 import workloads
+    from meanas_b200.operators import GridOperator
+    shape = tuple(args.shape) if args.shape else (160, 160, 128)
+    p = workloads.aniso_blocks(shape=shape)
+    dev = torch.device('cuda', 0)
+    op = GridOperator(p.omega, p.dxes, p.epsilon, device=dev, fp32=True)
+    J = torch.as_tensor(p.J, device=dev)
+    for method in ('cocg', 'mixed'):
+        _, info = op.solve(J, method=method, rtol=1e-30, maxiter=args.kernel_iters, criterion='true',
+                           profile=True, max_outer=1)
+        for k in range(4):
+            if info.kernel_count[k]:
+                ms = info.kernel_ms[k] / info.kernel_count[k]
+                gbs = KERNEL_BYTES_PER_CELL[k] * p.n_cells / (ms / 1e3) / 1e9
+                print(f'{method:6s} {KERNEL_NAMES[k]:20s} {info.kernel_count[k]:5d} launches  '
+                      f'{ms * 1e3:8.1f} us  {gbs:7.1f} GB/s algorithmic')
+    x = torch.randn(p.n_unknowns, dtype=torch.complex128, device=dev)
+    for prec, xx in (('c128', x), ('c64', x.to(torch.complex64))):
+        for _ in range(3):
+            op.apply(xx, precision=prec)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(10):
+            op.apply(xx, precision=prec)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / 10
+        per_cell = 6 * (16 if prec == 'c128' else 8) + 3 * (8 if prec == 'c128' else 4)
+        print(f'apply  A0_{prec:4s}               10 launches  {ms * 1e3:8.1f} us  '
+              f'{per_cell * p.n_cells / (ms / 1e3) / 1e9:7.1f} GB/s algorithmic')
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=5)
+    ap.add_argument('--steps', type=int, default=3)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', choices=['ours', 'reference'], default='ours')
-    ap.add_argument('--e2e-steps', type=int, default=3)
-    ap.add_argument('--cpu-sample-iters', type=int, default=8)
+    ap.add_argument('--e2e-steps', type=int, default=2)
+    ap.add_argument('--cpu-sample-iters', type=int, default=4)
     ap.add_argument('--ref-iters', type=int, default=3000,
                     help='QMR iterations per full solve used to extrapolate the reference arm')
+    ap.add_argument('--methods', default='mixed,cocg', help='GPU solvers to time (mixed, cocg)')
+    ap.add_argument('--kernel-iters', type=int, default=0,
+                    help='profiling mode: run this many iterations of each solver (no convergence, no JSON)')
+    ap.add_argument('--shape', type=int, nargs=3, default=None, help='profiling mode grid shape')
     args = ap.parse_args()
+    if args.kernel_iters > 0:
+        return kernel_mode(args)
     res = run_reference(args) if args.impl == 'reference' else run_ours(args)
     if res is not None:
         print(json.dumps(res), flush=True)

@@ -96,6 +96,8 @@ struct Geo {
   const cx<R>* idxh[3];  // 1/dx_h per axis
   const cx<R>* dxe[3];   // dx_e (for the symmetriser weights p^2)
   const cx<R>* dxh[3];
+  const R* adxe[3];      // |dx_e|, |dx_h|: |W| is a product of these (no square roots per cell)
+  const R* adxh[3];
   const R* eps;          // 3N
   const R* muinv;        // 3N or null
   const uint8_t* mask;   // N or null
@@ -112,18 +114,37 @@ __device__ __forceinline__ int wrapi(int v, int n) {
 template <typename R>
 struct WeightYZ {
   cx<R> yz[3];
+  R ayz[3];
   __device__ __forceinline__ void init(const Geo<R>& g, int j, int k) {
-    cx<R> ey = g.dxe[1][j], hy = g.dxh[1][j], ez = g.dxe[2][k], hz = g.dxh[2][k];
+    const cx<R> ey = g.dxe[1][j], hy = g.dxh[1][j], ez = g.dxe[2][k], hz = g.dxh[2][k];
     yz[0] = hy * hz;   // x: dxe_x * dxh_y * dxh_z
     yz[1] = ey * hz;   // y: dxh_x * dxe_y * dxh_z
     yz[2] = hy * ez;   // z: dxh_x * dxh_y * dxe_z
+    const R aey = g.adxe[1][j], ahy = g.adxh[1][j], aez = g.adxe[2][k], ahz = g.adxh[2][k];
+    ayz[0] = ahy * ahz;
+    ayz[1] = aey * ahz;
+    ayz[2] = ahy * aez;
   }
-  __device__ __forceinline__ void at(const Geo<R>& g, int i, cx<R> W[3]) const {
-    cx<R> ex = g.dxe[0][i], hx = g.dxh[0][i];
+  // W and |W| of the three components on plane i, from that plane's x factors
+  __device__ __forceinline__ void at(cx<R> ex, cx<R> hx, R aex, R ahx, cx<R> W[3], R aW[3]) const {
     W[0] = ex * yz[0];
     W[1] = hx * yz[1];
     W[2] = hx * yz[2];
+    aW[0] = aex * ayz[0];
+    aW[1] = ahx * ayz[1];
+    aW[2] = ahx * ayz[2];
   }
+};
+
+// Per-thread accumulators: FP64 for complex128 kernels, FP32 for complex64 kernels
+// (summed over one thread's cells; the CTA and grid sums are always FP64).
+template <typename R>
+struct AccT {
+  using type = double;
+};
+template <>
+struct AccT<float> {
+  using type = float;
 };
 
 // ---------------------------------------------------------------- reductions
@@ -155,13 +176,13 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
 
 // Reduce NRED per-thread accumulators across the grid; returns true in the one
 // thread (thread 0 of the last CTA) that holds the final sums in `out`.
-template <int NT, int NRED>
-__device__ bool grid_reduce(const double (&acc)[NRED], RedBuf rb, double* sh, double* out) {
+template <int NT, int NRED, typename A>
+__device__ bool grid_reduce(const A (&acc)[NRED], RedBuf rb, double* sh, double* out) {
   const int tid = threadIdx.x + threadIdx.y * blockDim.x;
   __shared__ bool s_last;
 #pragma unroll
   for (int r = 0; r < NRED; ++r) {
-    double s = block_sum<NT>(acc[r], sh);
+    double s = block_sum<NT>((double)acc[r], sh);
     if (tid == 0) rb.partials[(size_t)blockIdx.x * NRED + r] = s;
   }
   if (tid == 0) {
@@ -186,37 +207,79 @@ __device__ bool grid_reduce(const double (&acc)[NRED], RedBuf rb, double* sh, do
 
 // ---------------------------------------------------------------- stencil engine
 // Op interface:
-//   static constexpr int NRED;            number of FP64 accumulators (0 = none)
-//   static constexpr bool NEEDS_W;        pass symmetriser weights to own()
-//   bool skip() const;                    uniform early exit (solver stopped)
-//   void prepare();                       read scalars once per thread
-//   cx<R> load(int c, long long idx) const;   input field value (before PEC mask)
+//   static constexpr int NB;       box inputs: complex 3N vectors read on the tile + halo
+//   static constexpr int NS;       complex values per component stashed for own cells
+//   static constexpr int NRED;     number of FP64 accumulators (0 = none)
+//   static constexpr bool NEEDS_W; pass symmetriser weights to own()
+//   struct Pre;                    own-cell values prefetched at the start of a plane step
+//   bool skip() const;             uniform early exit (solver stopped)
+//   void prepare();                read scalars once per thread
+//   const cx<R>* box_src(int b) const;               null = zeros
+//   cx<R> make_u(const cx<R>* v, long long idx, int c) const;   input field from raw values
+//   void stash(const cx<R>* v, long long idx, int c, cx<R>* out) const;  own cell, NS values
+//   void pre(long long cell, Pre& p) const;
 //   void own(long long cell, int i, int j, int k, const cx<R> u[3], const cx<R> y[3],
-//            const cx<R> W[3], double* acc);   per own cell (u masked, y = A0 u)
+//            const cx<R> W[3], const cx<R>* st /*[3][NS]*/, const Pre& p, double* acc);
 //   void finish(const double* sums) const;    last CTA, thread 0
-template <typename R, int TZ, int TY, bool FLAT>
+//
+// Pipeline per x plane i (U holds u on planes i and i+1, Sbox the raw inputs of plane
+// i+2 in flight):  wait for plane i+1's copies -> convert them into U (u = make_u,
+// PEC mask; own cells also stash) -> issue cp.async for plane i+2 -> H = ce(u) on the
+// tile + low halo -> curl of H, epilogue.  Global loads of the box are asynchronous
+// copies, so they overlap the arithmetic of the previous plane.
+__device__ __forceinline__ void cp_async16(void* s, const void* g) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(g));
+}
+__device__ __forceinline__ void cp_async8(void* s, const void* g) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(g));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+template <typename R>
+__device__ __forceinline__ void cp_async_cx(cx<R>* s, const cx<R>* g) {
+  if constexpr (sizeof(cx<R>) == 16) cp_async16(s, g);
+  else cp_async8(s, g);
+}
+
+// Upper bound on x planes per CTA (per-CTA plane tables live in shared memory).
+constexpr int XC_MAX = 64;
+
+template <typename R, int TZ, int TY, bool FLAT, int NB, int NS>
 struct StencilShape {
   static constexpr int NT = TZ * TY;
   static constexpr int KZ = FLAT ? 0 : 1;      // z offset of own cells inside the box
   static constexpr int BW = TZ + 2 * KZ;       // box width (z)
   static constexpr int BH = TY + 2;            // box height (y)
   static constexpr int BOX = BW * BH;
-  static constexpr int NSLOT = (BOX + NT - 1) / NT;
+  static constexpr int NHALO = BOX - NT;       // halo cells (<= NT)
   static constexpr int HW = TZ + KZ;           // H plane width (own + low z halo)
   static constexpr int HH = TY + 1;
-  static constexpr size_t smem_bytes() {
-    return sizeof(cx<R>) * (2 * 3 * (size_t)BOX + 3 * (size_t)HW * HH) + 64 * sizeof(double);
-  }
+  // shared memory: Sbox[NB][3][BOX] | Sraw[2][NS][3][NT] | U[2][3][BOX] | Hs[3][HH*HW] | red[64]
+  static constexpr size_t off_raw = sizeof(cx<R>) * (size_t)NB * 3 * BOX;
+  static constexpr size_t off_u = off_raw + sizeof(cx<R>) * (size_t)2 * NS * 3 * NT;  // NS may be 0
+  static constexpr size_t off_h = off_u + sizeof(cx<R>) * (size_t)2 * 3 * BOX;
+  static constexpr size_t off_xt = off_h + sizeof(cx<R>) * (size_t)3 * HH * HW;
+  static constexpr int XT_STRIDE = 6;  // per plane: idxe, idxh, dxe, dxh, (|dxe|, |dxh|)
+  static constexpr size_t off_red = off_xt + sizeof(cx<R>) * (size_t)XT_STRIDE * (XC_MAX + 1);
+  static constexpr size_t smem_bytes() { return off_red + 64 * sizeof(double); }
+  static_assert(NHALO <= NT, "halo larger than the CTA");
 };
 
-template <typename R, int TZ, int TY, bool FLAT, class Op>
-__global__ void __launch_bounds__(TZ * TY) k_stencil(const Geo<R> g, Op op, RedBuf rb) {
-  using S = StencilShape<R, TZ, TY, FLAT>;
+template <typename R, int TZ, int TY, bool FLAT, int MINB, class Op>
+__global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op, RedBuf rb) {
+  using S = StencilShape<R, TZ, TY, FLAT, Op::NB, Op::NS>;
   constexpr int NT = S::NT, BW = S::BW, BOX = S::BOX, KZ = S::KZ, HW = S::HW, HH = S::HH;
+  constexpr int NB = Op::NB, NS = Op::NS > 0 ? Op::NS : 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  cx<R>* U = reinterpret_cast<cx<R>*>(smem_raw);             // [2][3][BOX]
-  cx<R>* Hs = U + 2 * 3 * BOX;                               // [3][HH*HW]
-  double* shred = reinterpret_cast<double*>(Hs + 3 * HH * HW);
+  cx<R>* Sbox = reinterpret_cast<cx<R>*>(smem_raw);                 // [NB][3][BOX]
+  cx<R>* Sraw = reinterpret_cast<cx<R>*>(smem_raw + S::off_raw);    // [2][NS][3][NT]
+  cx<R>* U = reinterpret_cast<cx<R>*>(smem_raw + S::off_u);         // [2][3][BOX]
+  cx<R>* Hs = reinterpret_cast<cx<R>*>(smem_raw + S::off_h);        // [3][HH*HW]
+  cx<R>* Xt = reinterpret_cast<cx<R>*>(smem_raw + S::off_xt);       // [XC+1][6]
+  double* shred = reinterpret_cast<double*>(smem_raw + S::off_red);
 
   if (op.skip()) return;
   Op o = op;
@@ -236,17 +299,28 @@ __global__ void __launch_bounds__(TZ * TY) k_stencil(const Geo<R> g, Op op, RedB
   const long long YZ = (long long)g.Y * g.Z;
   const long long N = g.N;
 
-  // box slots handled by this thread (constant over planes)
-  int slot_off[S::NSLOT];
-  int slot_pos[S::NSLOT];
-#pragma unroll
-  for (int s = 0; s < S::NSLOT; ++s) {
-    int bb = tid + s * NT;
-    slot_pos[s] = bb < BOX ? bb : -1;
-    int bj = bb / BW, bk = bb % BW;
-    int gj = wrapi(j0 - 1 + bj, g.Y);
-    int gk = FLAT ? 0 : wrapi(k0 - KZ + bk, g.Z);
-    slot_off[s] = gj * g.Z + gk;
+  // slot 0: this thread's own box cell; slot 1: one halo cell (or none)
+  const int pos0 = (ty + 1) * BW + tz + KZ;
+  const int off0 = wrapi(j0 + ty, g.Y) * g.Z + (FLAT ? 0 : wrapi(k0 + tz, g.Z));
+  int pos1 = -1, off1 = 0;
+  if (tid < S::NHALO) {
+    int bj, bk;
+    if (FLAT) {
+      bj = tid == 0 ? 0 : TY + 1;
+      bk = 0;
+    } else if (tid < BW) {
+      bj = 0;
+      bk = tid;
+    } else if (tid < 2 * BW) {
+      bj = TY + 1;
+      bk = tid - BW;
+    } else {
+      const int hh = tid - 2 * BW;
+      bj = 1 + hh / 2;
+      bk = (hh & 1) ? BW - 1 : 0;
+    }
+    pos1 = bj * BW + bk;
+    off1 = wrapi(j0 - 1 + bj, g.Y) * g.Z + (FLAT ? 0 : wrapi(k0 - KZ + bk, g.Z));
   }
 
   // per-thread y/z difference factors
@@ -254,30 +328,79 @@ __global__ void __launch_bounds__(TZ * TY) k_stencil(const Geo<R> g, Op op, RedB
   const cx<R> idze = FLAT ? czero<R>() : g.idxe[2][kc];
   const cx<R> idzh = FLAT ? czero<R>() : g.idxh[2][kc];
   const int jm = wrapi(j0 - 1, g.Y);
-  const cx<R> idye_jm = g.idxe[1][jm];
   const int km = FLAT ? 0 : wrapi(k0 - 1, g.Z);
+  const int kh = FLAT ? 0 : kc;
+  // the low-y halo row (j0-1) is computed by warp-row ty == 0, the low-z halo column
+  // (k0-1) by lanes tz < TY of the last warp-row (lane tz handles row j0 + tz)
+  const bool row_halo = (ty == 0);
+  const bool col_halo = !FLAT && (ty == TY - 1) && (tz < TY);
+  const int jr = wrapi(j0 + (col_halo ? tz : 0), g.Y);
+  const cx<R> idy_halo = row_halo ? g.idxe[1][jm] : (col_halo ? g.idxe[1][jr] : czero<R>());
   const cx<R> idze_km = FLAT ? czero<R>() : g.idxe[2][km];
-  const int kh = FLAT ? 0 : kc;  // z index used for halo-row H (row j0-1, own k)
+
+  // per-plane x factors of this CTA's planes (plane x0-1 first) into shared memory
+  for (int t = tid; t <= x1 - x0; t += NT) {
+    const int iw = wrapi(x0 - 1 + t, g.X);
+    cx<R>* e = Xt + t * S::XT_STRIDE;
+    e[0] = g.idxe[0][iw];
+    e[1] = g.idxh[0][iw];
+    e[2] = g.dxe[0][iw];
+    e[3] = g.dxh[0][iw];
+    e[4] = mkc<R>(g.adxe[0][iw], g.adxh[0][iw]);
+  }
 
   WeightYZ<R> wyz;
   if (Op::NEEDS_W) wyz.init(g, jc, kc);
 
-  double acc[Op::NRED > 0 ? Op::NRED : 1];
+  using A = typename AccT<R>::type;
+  A acc[Op::NRED > 0 ? Op::NRED : 1];
 #pragma unroll
-  for (int r = 0; r < (Op::NRED > 0 ? Op::NRED : 1); ++r) acc[r] = 0.0;
+  for (int r = 0; r < (Op::NRED > 0 ? Op::NRED : 1); ++r) acc[r] = A(0);
 
-  auto load_plane = [&](int buf, int iw) {
+  // issue the asynchronous copies of plane iw's box inputs into Sbox
+  auto issue = [&](int iw) {
     const long long base = (long long)iw * YZ;
 #pragma unroll
-    for (int s = 0; s < S::NSLOT; ++s) {
-      if (slot_pos[s] < 0) continue;
-      const long long cell = base + slot_off[s];
-      uint8_t m = g.mask ? g.mask[cell] : (uint8_t)0;
+    for (int bi = 0; bi < NB; ++bi) {
+      const cx<R>* src = o.box_src(bi);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        cx<R> v = o.load(c, c * N + cell);
-        if (m & (1u << c)) v = czero<R>();
-        U[(buf * 3 + c) * BOX + slot_pos[s]] = v;
+        cx<R>* dst = Sbox + (bi * 3 + c) * BOX;
+        if (src) {
+          cp_async_cx<R>(dst + pos0, src + c * N + base + off0);
+          if (pos1 >= 0) cp_async_cx<R>(dst + pos1, src + c * N + base + off1);
+        } else {
+          dst[pos0] = czero<R>();
+          if (pos1 >= 0) dst[pos1] = czero<R>();
+        }
+      }
+    }
+    cp_async_commit();
+  };
+  // convert the landed raw inputs of plane iw into U[buf] (and stash own cells)
+  auto convert = [&](int buf, int iw, int sb) {  // sb: stash buffer (-1 = none)
+    const long long base = (long long)iw * YZ;
+#pragma unroll
+    for (int sl = 0; sl < 2; ++sl) {
+      const int pos = sl == 0 ? pos0 : pos1;
+      if (pos < 0) continue;
+      const long long cell = base + (sl == 0 ? off0 : off1);
+      const uint8_t m = g.mask ? g.mask[cell] : (uint8_t)0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        cx<R> v[NB > 0 ? NB : 1];
+#pragma unroll
+        for (int bi = 0; bi < NB; ++bi) v[bi] = Sbox[(bi * 3 + c) * BOX + pos];
+        const long long idx = c * N + cell;
+        cx<R> u = o.make_u(v, idx, c);
+        if (m & (1u << c)) u = czero<R>();
+        U[(buf * 3 + c) * BOX + pos] = u;
+        if (Op::NS > 0 && sl == 0 && sb >= 0) {
+          cx<R> st[NS];
+          o.stash(v, idx, c, st);
+#pragma unroll
+          for (int q = 0; q < Op::NS; ++q) Sraw[((sb * NS + q) * 3 + c) * NT + tid] = st[q];
+        }
       }
     }
   };
@@ -290,7 +413,7 @@ __global__ void __launch_bounds__(TZ * TY) k_stencil(const Geo<R> g, Op op, RedB
       hz = g.muinv[2 * N + cell] * hz;
     }
     if (g.mask) {
-      uint8_t m = g.mask[cell];
+      const uint8_t m = g.mask[cell];
       if (m & 8u) hx = czero<R>();
       if (m & 16u) hy = czero<R>();
       if (m & 32u) hz = czero<R>();
@@ -322,15 +445,24 @@ __global__ void __launch_bounds__(TZ * TY) k_stencil(const Geo<R> g, Op op, RedB
     }
   };
 
-  // ---- prologue: H on plane x0-1 (own cells; only Hy, Hz are needed downstream)
+  // ---- prologue: planes x0-1 and x0 into U, H on plane x0-1 (own cells: Hy, Hz)
   const int ip = wrapi(x0 - 1, g.X);
-  load_plane(0, ip);
-  load_plane(1, x0);
+  issue(ip);
+  cp_async_wait_all();
   __syncthreads();
+  convert(0, ip, -1);
+  __syncthreads();
+  issue(x0);
+  cp_async_wait_all();
+  __syncthreads();
+  convert(1, x0, 0);
+  __syncthreads();
+  // plane x0+1 starts landing while the prologue H is computed
+  issue(x0 + 1 == g.X ? 0 : x0 + 1);
   cx<R> hy_prev, hz_prev;
   {
     cx<R> hx, hy, hz;
-    curl_e(0, 1, ty + 1, tz + KZ, idye, idze, g.idxe[0][ip], hx, hy, hz);
+    curl_e(0, 1, ty + 1, tz + KZ, idye, idze, Xt[0], hx, hy, hz);
     hscale((long long)ip * YZ + (long long)jc * g.Z + kc, hx, hy, hz);
     hy_prev = hy;
     hz_prev = hz;
@@ -338,47 +470,52 @@ __global__ void __launch_bounds__(TZ * TY) k_stencil(const Geo<R> g, Op op, RedB
   int cur = 1;
   for (int i = x0; i < x1; ++i) {
     const int nxt = cur ^ 1;
-    const int in = (i + 1 == g.X) ? 0 : i + 1;
-    __syncthreads();  // everyone is done reading buffer `nxt` (plane i-1) and Hs
-    load_plane(nxt, in);
-    __syncthreads();
-    const cx<R> idxe_i = g.idxe[0][i], idxh_i = g.idxh[0][i];
+    const int in1 = (i + 1 == g.X) ? 0 : i + 1;
     const long long ibase = (long long)i * YZ;
-    // own H
+    const long long cell = ibase + (long long)jc * g.Z + kc;
+    // own-cell prefetch for this plane's epilogue (latency hidden by the H pass)
+    typename Op::Pre pr;
+    R e3[3];
+    if (active) {
+      o.pre(cell, pr);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) e3[c] = g.eps[c * N + cell];
+    }
+    cp_async_wait_all();   // plane i+1 landed
+    __syncthreads();       // ... for everyone; U[nxt] (plane i-1) and Hs no longer read
+    convert(nxt, in1, (i + 1 - x0) & 1);
+    __syncthreads();       // U[nxt] = u(i+1) ready; Sbox free
+    if (i + 1 < x1) issue(in1 + 1 == g.X ? 0 : in1 + 1);
+    const cx<R>* xe = Xt + (i - x0 + 1) * S::XT_STRIDE;
+    const cx<R> idxe_i = xe[0], idxh_i = xe[1];
     cx<R> hx, hy, hz;
     curl_e(cur, nxt, ty + 1, tz + KZ, idye, idze, idxe_i, hx, hy, hz);
-    hscale(ibase + (long long)jc * g.Z + kc, hx, hy, hz);
+    hscale(cell, hx, hy, hz);
     const int hp = (ty + 1) * HW + tz + KZ;
     Hs[0 * HH * HW + hp] = hx;
     Hs[1 * HH * HW + hp] = hy;
     Hs[2 * HH * HW + hp] = hz;
-    // low y halo row (j0-1)
-    if (ty == 0) {
+    if (row_halo) {  // low y halo row (j0-1)
       cx<R> ax, ay, az;
-      curl_e(cur, nxt, 0, tz + KZ, idye_jm, idze, idxe_i, ax, ay, az);
+      curl_e(cur, nxt, 0, tz + KZ, idy_halo, idze, idxe_i, ax, ay, az);
       hscale(ibase + (long long)jm * g.Z + kh, ax, ay, az);
       Hs[0 * HH * HW + tz + KZ] = ax;
       Hs[1 * HH * HW + tz + KZ] = ay;
       Hs[2 * HH * HW + tz + KZ] = az;
     }
-    // low z halo column (k0-1)
-    if (!FLAT && tz == 0) {
+    if (col_halo) {  // low z halo column (k0-1), row j0 + tz
       cx<R> ax, ay, az;
-      curl_e(cur, nxt, ty + 1, 0, idye, idze_km, idxe_i, ax, ay, az);
-      hscale(ibase + (long long)jc * g.Z + km, ax, ay, az);
-      Hs[0 * HH * HW + (ty + 1) * HW] = ax;
-      Hs[1 * HH * HW + (ty + 1) * HW] = ay;
-      Hs[2 * HH * HW + (ty + 1) * HW] = az;
+      curl_e(cur, nxt, tz + 1, 0, idy_halo, idze_km, idxe_i, ax, ay, az);
+      hscale(ibase + (long long)jr * g.Z + km, ax, ay, az);
+      Hs[0 * HH * HW + (tz + 1) * HW] = ax;
+      Hs[1 * HH * HW + (tz + 1) * HW] = ay;
+      Hs[2 * HH * HW + (tz + 1) * HW] = az;
     }
     cx<R> u[3];
-    {
-      const int p = (ty + 1) * BW + tz + KZ;
-      u[0] = U[(cur * 3 + 0) * BOX + p];
-      u[1] = U[(cur * 3 + 1) * BOX + p];
-      u[2] = U[(cur * 3 + 2) * BOX + p];
-    }
+    u[0] = U[(cur * 3 + 0) * BOX + pos0];
+    u[1] = U[(cur * 3 + 1) * BOX + pos0];
+    u[2] = U[(cur * 3 + 2) * BOX + pos0];
     __syncthreads();
-    // curl of H on own cells
     const cx<R> hz_jm = Hs[2 * HH * HW + ty * HW + tz + KZ];
     const cx<R> hx_jm = Hs[0 * HH * HW + ty * HW + tz + KZ];
     cx<R> y[3];
@@ -395,21 +532,28 @@ __global__ void __launch_bounds__(TZ * TY) k_stencil(const Geo<R> g, Op op, RedB
     hy_prev = hy;
     hz_prev = hz;
     if (active) {
-      const long long cell = ibase + (long long)j * g.Z + k;
       const uint8_t m = g.mask ? g.mask[cell] : (uint8_t)0;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const R e = g.eps[c * N + cell];
-        cx<R> v = y[c] - (e * g.w2) * u[c];
+        cx<R> v = y[c] - (e3[c] * g.w2) * u[c];
         if (m & (1u << c)) v = czero<R>();
         y[c] = v;
       }
       cx<R> W[3];
-      if (Op::NEEDS_W) wyz.at(g, i, W);
-      o.own(cell, i, j, k, u, y, W, acc);
+      R aW[3];
+      if (Op::NEEDS_W) wyz.at(xe[2], xe[3], xe[4].re, xe[4].im, W, aW);
+      cx<R> st[3 * NS];
+      if (Op::NS > 0) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int q = 0; q < Op::NS; ++q) st[c * NS + q] = Sraw[((((i - x0) & 1) * NS + q) * 3 + c) * NT + tid];
+      }
+      o.own(cell, i, j, k, u, y, W, aW, st, pr, acc);
     }
     cur = nxt;
   }
+  cp_async_wait_all();
 
   if constexpr (Op::NRED > 0) {
     double sums[Op::NRED];
@@ -438,14 +582,17 @@ __global__ void __launch_bounds__(TZ * TY) k_point(const Geo<R> g, Op op, RedBuf
   const long long YZ = (long long)g.Y * g.Z;
   WeightYZ<R> wyz;
   if (Op::NEEDS_W) wyz.init(g, min(j, g.Y - 1), min(k, g.Z - 1));
-  double acc[Op::NRED > 0 ? Op::NRED : 1];
+  using A = typename AccT<R>::type;
+  A acc[Op::NRED > 0 ? Op::NRED : 1];
 #pragma unroll
-  for (int r = 0; r < (Op::NRED > 0 ? Op::NRED : 1); ++r) acc[r] = 0.0;
+  for (int r = 0; r < (Op::NRED > 0 ? Op::NRED : 1); ++r) acc[r] = A(0);
   if (active) {
+#pragma unroll 2
     for (int i = x0; i < x1; ++i) {
       cx<R> W[3];
-      if (Op::NEEDS_W) wyz.at(g, i, W);
-      o.point((long long)i * YZ + (long long)j * g.Z + k, i, j, k, W, acc);
+      R aW[3];
+      if (Op::NEEDS_W) wyz.at(g.dxe[0][i], g.dxh[0][i], g.adxe[0][i], g.adxh[0][i], W, aW);
+      o.point((long long)i * YZ + (long long)j * g.Z + k, i, j, k, W, aW, acc);
     }
   }
   if constexpr (Op::NRED > 0) {

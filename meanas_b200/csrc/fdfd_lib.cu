@@ -68,9 +68,9 @@ __global__ void k_to_f32(const double* src, float* dst, long long n) {
     dst[i] = (float)src[i];
 }
 
-// 1D tables: copies of dx, and 1/dx (given, or computed with a scaled complex division)
-__global__ void k_tables(const double2* dx, const double2* inv_given, double2* dx64, double2* inv64,
-                         float2* dx32, float2* inv32, int n) {
+// 1D tables: copies of dx, |dx|, and 1/dx (given, or computed with a scaled complex division)
+__global__ void k_tables(const double2* dx, const double2* inv_given, double2* dx64, double2* inv64, double* abs64,
+                         float2* dx32, float2* inv32, float* abs32, int n) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double2 d = dx[i];
     double2 r;
@@ -82,9 +82,11 @@ __global__ void k_tables(const double2* dx, const double2* inv_given, double2* d
     }
     dx64[i] = d;
     inv64[i] = r;
+    abs64[i] = hypot(d.x, d.y);
     if (dx32) {
       dx32[i] = make_float2((float)d.x, (float)d.y);
       inv32[i] = make_float2((float)r.x, (float)r.y);
+      abs32[i] = (float)abs64[i];
     }
   }
 }
@@ -166,6 +168,17 @@ static void prof_collect(fdfd_plan* P, double* ms, int* cnt) {
 }
 
 static constexpr int FLAT_TY = 256;
+
+// Resident CTAs per SM the stencil kernels are compiled for (register cap 65536 /
+// (256 threads x value)): complex64 passes carry less state than complex128 ones.
+template <typename R>
+struct MinBlocks {
+  static constexpr int value = 2;
+};
+template <>
+struct MinBlocks<float> {
+  static constexpr int value = 3;
+};
 static constexpr int TZ3 = 32, TY3 = 8;
 
 static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
@@ -183,7 +196,7 @@ static Tiling make_tiling(const fdfd_plan* P, int precision) {
     long long need = (P->X * tiles + target - 1) / target;
     xc = (int)std::max(4LL, std::min(64LL, need));
   }
-  xc = std::min(xc, P->X);
+  xc = std::min(std::min(xc, P->X), XC_MAX);
   t.XC = xc;
   t.nxc = (P->X + xc - 1) / xc;
   t.nblocks = tiles * t.nxc;
@@ -227,13 +240,13 @@ static int launch_stencil(fdfd_plan* P, const Geo<R>& g0, int precision, const O
   const Tiling t = make_tiling(P, precision);
   const Geo<R> g = geo_with(g0, t);
   if (P->flat) {
-    using Sh = StencilShape<R, 1, FLAT_TY, true>;
-    auto kern = k_stencil<R, 1, FLAT_TY, true, Op>;
+    using Sh = StencilShape<R, 1, FLAT_TY, true, Op::NB, Op::NS>;
+    auto kern = k_stencil<R, 1, FLAT_TY, true, MinBlocks<R>::value, Op>;
     ensure_smem(kern, Sh::smem_bytes());
     kern<<<(unsigned)t.nblocks, dim3(1, FLAT_TY), Sh::smem_bytes(), s>>>(g, op, rb);
   } else {
-    using Sh = StencilShape<R, TZ3, TY3, false>;
-    auto kern = k_stencil<R, TZ3, TY3, false, Op>;
+    using Sh = StencilShape<R, TZ3, TY3, false, Op::NB, Op::NS>;
+    auto kern = k_stencil<R, TZ3, TY3, false, MinBlocks<R>::value, Op>;
     ensure_smem(kern, Sh::smem_bytes());
     kern<<<(unsigned)t.nblocks, dim3(TZ3, TY3), Sh::smem_bytes(), s>>>(g, op, rb);
   }
@@ -289,9 +302,9 @@ static int plan_layout(const fdfd_grid_desc* d, PlanLayout* L) {
   L->mask = off;
   if (d->pec || d->pmc) off += align256((size_t)N);
   L->tab64 = off;
-  off += align256(4 * S * sizeof(double2));
+  off += align256(4 * S * sizeof(double2) + 2 * S * sizeof(double));
   L->tab32 = off;
-  if (f32) off += align256(4 * S * sizeof(float2));
+  if (f32) off += align256(4 * S * sizeof(float2) + 2 * S * sizeof(float));
   L->total = off;
   return 0;
 }
@@ -350,27 +363,37 @@ extern "C" int fdfd_plan_create(const fdfd_grid_desc* d, void* ws, size_t ws_byt
   float2* t32 = P->has32 ? (float2*)(base + L.tab32) : nullptr;
   const long long S = (long long)P->X + P->Y + P->Z;
   long long aoff = 0;
+  double* a64 = (double*)(t64 + 4 * S);
+  float* a32 = t32 ? (float*)(t32 + 4 * S) : nullptr;
   for (int a = 0; a < 3; ++a) {
     double2* dxe64 = t64 + aoff;
     double2* dxh64 = t64 + S + aoff;
     double2* ie64 = t64 + 2 * S + aoff;
     double2* ih64 = t64 + 3 * S + aoff;
+    double* ae64 = a64 + aoff;
+    double* ah64 = a64 + S + aoff;
     float2* dxe32 = t32 ? t32 + aoff : nullptr;
     float2* dxh32 = t32 ? t32 + S + aoff : nullptr;
     float2* ie32 = t32 ? t32 + 2 * S + aoff : nullptr;
     float2* ih32 = t32 ? t32 + 3 * S + aoff : nullptr;
+    float* ae32 = a32 ? a32 + aoff : nullptr;
+    float* ah32 = a32 ? a32 + S + aoff : nullptr;
     k_tables<<<(sh[a] + 255) / 256, 256, 0, s>>>((const double2*)d->dxe[a], (const double2*)d->inv_dxe[a], dxe64,
-                                                 ie64, dxe32, ie32, sh[a]);
+                                                 ie64, ae64, dxe32, ie32, ae32, sh[a]);
     k_tables<<<(sh[a] + 255) / 256, 256, 0, s>>>((const double2*)d->dxh[a], (const double2*)d->inv_dxh[a], dxh64,
-                                                 ih64, dxh32, ih32, sh[a]);
+                                                 ih64, ah64, dxh32, ih32, ah32, sh[a]);
     P->g64.dxe[a] = (const cx<double>*)dxe64;
     P->g64.dxh[a] = (const cx<double>*)dxh64;
     P->g64.idxe[a] = (const cx<double>*)ie64;
     P->g64.idxh[a] = (const cx<double>*)ih64;
+    P->g64.adxe[a] = ae64;
+    P->g64.adxh[a] = ah64;
     P->g32.dxe[a] = (const cx<float>*)dxe32;
     P->g32.dxh[a] = (const cx<float>*)dxh32;
     P->g32.idxe[a] = (const cx<float>*)ie32;
     P->g32.idxh[a] = (const cx<float>*)ih32;
+    P->g32.adxe[a] = ae32;
+    P->g32.adxh[a] = ah32;
     aoff += sh[a];
   }
   const int nb = (int)std::min<long long>((3 * N + 255) / 256, 148LL * 16);
@@ -584,7 +607,7 @@ static int graph_batch(fdfd_plan* P, int kind, const void* ka, const void* kb, i
     }
   }
   cudaGraph_t g;
-  CK(cudaStreamBeginCapture(P->cap, cudaStreamCaptureModeThreadLocal));
+  CK(cudaStreamBeginCapture(P->cap, cudaStreamCaptureModeRelaxed));
   const int saved = P->launches;
   int rc = enqueue(P->cap);
   P->launches = saved;
@@ -650,7 +673,7 @@ static int refine_loop(SolveCtx& c, const Geo<RI>& gi, int prec, BsBufs B, doubl
   for (;;) {
     // the shadow seed is baked into captured graphs, which are keyed by local_outer % 8
     const unsigned long long seed = 0x5eed5eedULL + 0x9e3779b97f4a7c15ULL * (unsigned long long)(local_outer % 8);
-    OpRefine<RI> rf{Ecur, have_d ? D : nullptr, Enext, c.b, (cx<RI>*)B.R[0], c.bnorm, rscale, N, seed, c.st};
+    OpRefine<RI> rf{Ecur, have_d ? D : nullptr, Enext, c.b, (cx<RI>*)B.R0, c.bnorm, rscale, N, seed, c.st};
     TRY(launch_stencil<double>(P, P->g64, 0, rf, c.rb, s));
     std::swap(Ecur, Enext);
     CK(cudaMemcpyAsync(P->h_state, c.st, sizeof(KState), cudaMemcpyDeviceToHost, s));
@@ -746,12 +769,12 @@ extern "C" int fdfd_solve(fdfd_plan* P, const fdfd_solve_opts* o, const void* J,
   c.status = ST_RUNNING;
   const int maxiter = o->maxiter;
   BsBufs B;
-  B.R[0] = base + L.inner[0];
-  B.R[1] = base + L.inner[1];
-  B.V[0] = base + L.inner[2];
-  B.V[1] = base + L.inner[3];
-  B.P[0] = base + L.inner[4];
-  B.P[1] = base + L.inner[5];
+  B.R0 = base + L.inner[0];
+  B.R1 = base + L.inner[1];
+  B.V0 = base + L.inner[2];
+  B.V1 = base + L.inner[3];
+  B.P0 = base + L.inner[4];
+  B.P1 = base + L.inner[5];
   B.T = base + L.inner[6];
   B.x = base + L.inner[7];
 
@@ -782,7 +805,7 @@ extern "C" int fdfd_solve(fdfd_plan* P, const fdfd_solve_opts* o, const void* J,
     cx<double>* P1 = (cx<double>*)(base + L.cocg[3]);
     CK(cudaMemsetAsync(P0, 0, vbytes128, s));
     {
-      OpCocgInit<double> op{c.b, o->has_guess ? c.x : nullptr, r, N, c.st};
+      OpCocgInit<double> op{c.b, o->has_guess ? c.x : nullptr, r, N, c.st, 0.0, 0ULL, nullptr};
       TRY(launch_stencil<double>(P, P->g64, 0, op, c.rb, s));
     }
     KState* st = c.st;
@@ -804,24 +827,59 @@ extern "C" int fdfd_solve(fdfd_plan* P, const fdfd_solve_opts* o, const void* J,
       }
       return 0;
     };
-    if (maxiter > 0) {
-      TRY(drive(P, st, chunk, maxiter, s, [&]() -> int {
-        if (o->use_graph && !P->profiling) {
-          P->launches += 2 * chunk;
-          return graph_batch(P, 0, ws, E, chunk, s, enqueue);
-        }
-        return enqueue(s);
-      }));
+    int restarts = 0;
+    for (;;) {
+      CK(cudaMemcpyAsync(P->h_state, st, sizeof(KState), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      const int left = maxiter - c.iters;
+      if (P->h_state->status == ST_RUNNING && left > 0) {
+        TRY(drive(P, st, chunk, left, s, [&]() -> int {
+          if (o->use_graph && !P->profiling) {
+            P->launches += 2 * chunk;
+            return graph_batch(P, 0, ws, E, chunk, s, enqueue);
+          }
+          return enqueue(s);
+        }));
+      }
+      OpCocgFinal<double> fin{P0, P1, x, N, st};
+      TRY(launch_point<double>(P, P->g64, 0, fin, rb, s));
+      CK(cudaMemcpyAsync(P->h_state, st, sizeof(KState), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      c.iters += P->h_state->iter;
+      c.status = P->h_state->status;
+      if (c.status == ST_RUNNING) c.status = ST_MAXITER;
+      if (c.status != ST_BREAKDOWN || restarts >= 8 || c.iters >= maxiter) break;
+      // Breakdown: the unconjugated form cancelled (for example a source whose
+      // r^T W r is exactly zero).  Restart COCG from x + s xi, xi a hashed random
+      // vector with |A0 s xi| = 0.1 |r|, which makes the new residual generic.
+      ++restarts;
+      const double rr_before = std::max(P->h_state->rr, 1e-300);
+      const unsigned long long seed = 0xc0c6ULL + 0x9e3779b97f4a7c15ULL * (unsigned long long)restarts;
+      {
+        OpCocgInit<double> probe{nullptr, nullptr, q, N, st, 1.0, seed, nullptr};
+        TRY(launch_stencil<double>(P, P->g64, 0, probe, rb, s));
+      }
+      CK(cudaMemcpyAsync(P->h_state, st, sizeof(KState), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      const double axi = std::sqrt(std::max(P->h_state->rr, 1e-300));
+      const double scale = 0.1 * std::sqrt(rr_before) / axi;
+      {
+        OpCocgInit<double> op{c.b, x, r, N, st, scale, seed, c.e2};
+        TRY(launch_stencil<double>(P, P->g64, 0, op, rb, s));
+      }
+      CK(cudaMemcpyAsync(x, c.e2, vbytes128, cudaMemcpyDeviceToDevice, s));
+      CK(cudaMemsetAsync(P0, 0, vbytes128, s));
+      // the restarted sequence counts on from c.iters: shift its cap and history
+      KState* hs = P->h_state;
+      CK(cudaMemcpyAsync(hs, st, sizeof(KState), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      hs->maxiter = maxiter - c.iters;
+      hs->hist = o->history ? o->history + c.iters : nullptr;
+      CK(cudaMemcpyAsync(st, hs, sizeof(KState), cudaMemcpyHostToDevice, s));
     }
-    OpCocgFinal<double> fin{P0, P1, x, N, st};
-    TRY(launch_point<double>(P, P->g64, 0, fin, rb, s));
-    CK(cudaMemcpyAsync(P->h_state, st, sizeof(KState), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    c.iters = P->h_state->iter;
-    c.status = P->h_state->status;
     if (c.status == ST_BREAKDOWN || c.status == ST_NONFINITE) {
-      // COCG broke down (the unconjugated form cancelled): continue from the
-      // current iterate with complex128 BiCGSTAB inside the refinement loop.
+      // still stuck: continue from the current iterate with complex128 BiCGSTAB
+      // inside the refinement loop (restarting with fresh shadow vectors).
       if (c.status == ST_NONFINITE) CK(cudaMemsetAsync(E, 0, vbytes128, s));
       c.status = ST_RUNNING;
       TRY(refine_loop<double>(c, P->g64, 0, B, 1e-10, 64, 2));

@@ -85,11 +85,31 @@ __device__ __forceinline__ void check_progress(KState* st, double monitored, boo
   }
 }
 
-// |W| for the three components (magnitudes multiply, so no square root per cell).
 template <typename R>
-__device__ __forceinline__ void absW3(const cx<R> W[3], R a[3]) {
-#pragma unroll
-  for (int c = 0; c < 3; ++c) a[c] = sqrt(cabs2(W[c]));
+using acc_t = typename AccT<R>::type;
+
+// ------------------------------------------------------------------ hashed random vectors
+__device__ __forceinline__ unsigned hash32(unsigned x) {
+  x ^= x >> 16;
+  x *= 0x7feb352dU;
+  x ^= x >> 15;
+  x *= 0x846ca68bU;
+  x ^= x >> 16;
+  return x;
+}
+// Element idx of a fixed pseudo-random complex vector (components in [-1/2, 1/2)):
+// BiCGSTAB's shadow vector and the restart perturbation, with no memory traffic.
+template <typename R>
+__device__ __forceinline__ cx<R> shadow(long long idx, unsigned long long seed) {
+  const unsigned a = hash32((unsigned)idx ^ (unsigned)seed);
+  const unsigned b = hash32(a ^ (unsigned)(seed >> 32) ^ 0x9e3779b9U);
+  return mkc<R>((R)a * (R)2.3283064365386963e-10 - (R)0.5, (R)b * (R)2.3283064365386963e-10 - (R)0.5);
+}
+// conj(a) * b added to two accumulators of precision A
+template <typename R, typename A>
+__device__ __forceinline__ void acc_cdot(A* acc, cx<R> a, cx<R> b) {
+  acc[0] += (A)a.re * (A)b.re + (A)a.im * (A)b.im;
+  acc[1] += (A)a.re * (A)b.im - (A)a.im * (A)b.re;
 }
 
 // ------------------------------------------------------------------ plain operator
@@ -110,14 +130,17 @@ __device__ __forceinline__ dcx csqrt_principal(dcx z) {
 
 template <typename R>
 struct OpApply {
-  static constexpr int NRED = 0;
-  static constexpr bool NEEDS_W = true;
+  static constexpr int NB = 1, NS = 0, NRED = 0;
+  static constexpr bool NEEDS_W = false;
   const cx<R>* x;
   cx<R>* y;
   int mode;
   Geo<R> g;
+  struct Pre {};
   __device__ bool skip() const { return false; }
   __device__ void prepare() {}
+  __device__ const cx<R>* box_src(int) const { return x; }
+  __device__ void pre(long long, Pre&) const {}
   __device__ cx<R> pl_at(int c, long long idx) const {
     const long long N = g.N;
     const long long cell = idx - c * N;
@@ -132,20 +155,20 @@ struct OpApply {
     dcx s = csqrt_principal({(double)p2.re, (double)p2.im});
     return mkc<R>((R)s.re, (R)s.im);
   }
-  __device__ cx<R> load(int c, long long idx) const {
-    cx<R> v = x[idx];
-    if (mode == 2) v = cconj(v);
+  __device__ cx<R> make_u(const cx<R>* v, long long idx, int c) const {
+    cx<R> u = v[0];
+    if (mode == 2) u = cconj(u);
     if (mode >= 1) {
       const cx<R> pl = pl_at(c, idx);
       // Pr = 1 / Pl
       const R d = cabs2(pl);
-      const cx<R> pr = mkc<R>(pl.re / d, -pl.im / d);
-      v = v * pr;
+      u = u * mkc<R>(pl.re / d, -pl.im / d);
     }
-    return v;
+    return u;
   }
-  __device__ void own(long long cell, int, int, int, const cx<R>*, const cx<R> yv[3], const cx<R>*,
-                      double*) const {
+  __device__ void stash(const cx<R>*, long long, int, cx<R>*) const {}
+  __device__ void own(long long cell, int, int, int, const cx<R>*, const cx<R> yv[3], const cx<R>*, const R*,
+                      const cx<R>*, const Pre&, acc_t<R>*) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const long long idx = c * g.N + cell;
@@ -179,10 +202,8 @@ struct OpRhs {
   KState* st;
   __device__ bool skip() const { return false; }
   __device__ void prepare() {}
-  __device__ void point(long long cell, int, int, int, const cx<R> W[3], double* acc) const {
+  __device__ void point(long long cell, int, int, int, const cx<R> W[3], const R aW[3], acc_t<R>* acc) const {
     const uint8_t m = mask ? mask[cell] : (uint8_t)0;
-    R aW[3];
-    absW3<R>(W, aW);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const long long idx = c * N + cell;
@@ -228,7 +249,7 @@ struct OpAdjPost {
   long long N;
   __device__ bool skip() const { return false; }
   __device__ void prepare() {}
-  __device__ void point(long long cell, int, int, int, const cx<R> W[3], double*) const {
+  __device__ void point(long long cell, int, int, int, const cx<R> W[3], const R*, acc_t<R>*) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const long long idx = c * N + cell;
@@ -239,28 +260,45 @@ struct OpAdjPost {
 };
 
 // ------------------------------------------------------------------ COCG
-// init: r = b - A0 x0 (x0 may be zero); reduces r^T W r, |r|^2, sum|W||r|^2, sum|W|^2|r|^2
+// init: u = x0 + pert * xi (x0 may be zero; xi a hashed random vector used to restart
+// after a breakdown), r = b - A0 u (b may be zero), optionally x_new = u;
+// reduces r^T W r, |r|^2, sum|W||r|^2, sum|W|^2|r|^2.
 template <typename R>
 struct OpCocgInit {
-  static constexpr int NRED = 5;
+  static constexpr int NB = 1, NS = 0, NRED = 5;
   static constexpr bool NEEDS_W = true;
-  const cx<R>* b;
-  const cx<R>* x;  // may be null (zero guess)
+  const cx<R>* b;   // may be null (zero)
+  const cx<R>* x;   // may be null (zero guess)
   cx<R>* r;
   long long N;
   KState* st;
+  double pert;
+  unsigned long long seed;
+  cx<R>* xnew;      // may be null
+  struct Pre {
+    cx<R> b[3];
+  };
   __device__ bool skip() const { return false; }
   __device__ void prepare() {}
-  __device__ cx<R> load(int, long long idx) const { return x ? x[idx] : czero<R>(); }
-  __device__ void own(long long cell, int, int, int, const cx<R>*, const cx<R> y[3], const cx<R> W[3],
-                      double* acc) const {
-    R aW[3];
-    absW3<R>(W, aW);
+  __device__ const cx<R>* box_src(int) const { return x; }
+  __device__ void pre(long long cell, Pre& p) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) p.b[c] = b ? b[c * N + cell] : czero<R>();
+  }
+  __device__ cx<R> make_u(const cx<R>* v, long long idx, int) const {
+    cx<R> u = v[0];
+    if (pert != 0.0) u = caxpy(mkc<R>((R)pert, R(0)), shadow<R>(idx, seed), u);
+    return u;
+  }
+  __device__ void stash(const cx<R>*, long long, int, cx<R>*) const {}
+  __device__ void own(long long cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R> W[3],
+                      const R aW[3], const cx<R>*, const Pre& pr, acc_t<R>* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const long long idx = c * N + cell;
-      const cx<R> rv = b[idx] - y[c];
+      const cx<R> rv = pr.b[c] - y[c];
       r[idx] = rv;
+      if (xnew) xnew[idx] = u[c];
       const cx<R> wr = W[c] * rv;
       acc[0] += (double)wr.re * (double)rv.re - (double)wr.im * (double)rv.im;
       acc[1] += (double)wr.re * (double)rv.im + (double)wr.im * (double)rv.re;
@@ -289,7 +327,7 @@ struct OpCocgInit {
 // p = r + beta p_old ; x += alpha p_old (deferred) ; q = A0 p ; sigma = p^T W q
 template <typename R>
 struct OpCocgA {
-  static constexpr int NRED = 4;
+  static constexpr int NB = 2, NS = 1, NRED = 2;
   static constexpr bool NEEDS_W = true;
   const cx<R>* r;
   cx<R>* P0;
@@ -303,6 +341,9 @@ struct OpCocgA {
   cx<R>* p_new;
   cx<R> beta, alpha;
   bool upd;
+  struct Pre {
+    cx<R> x[3];
+  };
   __device__ bool skip() const { return ld_status(st) != ST_RUNNING; }
   __device__ void prepare() {
     const int k = __ldcg(&st->iter);
@@ -312,21 +353,25 @@ struct OpCocgA {
     alpha = from_d<R>(ld_dcx(&st->alpha));
     upd = __ldcg(&st->pending) != 0;
   }
-  __device__ cx<R> load(int, long long idx) const { return caxpy(beta, p_old[idx], r[idx]); }
+  __device__ const cx<R>* box_src(int bi) const { return bi == 0 ? r : p_old; }
+  __device__ void pre(long long cell, Pre& p) const {
+    if (!upd) return;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) p.x[c] = x[c * N + cell];
+  }
+  __device__ cx<R> make_u(const cx<R>* v, long long, int) const { return caxpy(beta, v[1], v[0]); }
+  __device__ void stash(const cx<R>* v, long long, int, cx<R>* out) const { out[0] = v[1]; }
   __device__ void own(long long cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R> W[3],
-                      double* acc) const {
+                      const R*, const cx<R>* sv, const Pre& pr, acc_t<R>* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const long long idx = c * N + cell;
-      if (upd) x[idx] = caxpy(alpha, p_old[idx], x[idx]);
+      if (upd) x[idx] = caxpy(alpha, sv[c], pr.x[c]);
       p_new[idx] = u[c];
       q[idx] = y[c];
       const cx<R> wp = W[c] * u[c];
       acc[0] += (double)wp.re * (double)y[c].re - (double)wp.im * (double)y[c].im;
       acc[1] += (double)wp.re * (double)y[c].im + (double)wp.im * (double)y[c].re;
-      const double aw = (double)sqrt(cabs2(W[c]));
-      acc[2] += aw * (double)cabs2(u[c]);
-      acc[3] += aw * (double)cabs2(y[c]);
     }
   }
   __device__ void finish(const double* s) const {
@@ -337,8 +382,9 @@ struct OpCocgA {
       st->status = ST_NONFINITE;
       return;
     }
-    // |p^T W q| <= ||p||_|W| ||q||_|W|; a ratio below 1e-14 is a (near) breakdown
-    if (dabs(sigma) <= BREAKDOWN_RATIO * sqrt(s[2] * s[3])) {
+    // an exactly vanishing p^T W q; near-vanishing values are caught by the residual
+    // blow-up test of the pointwise pass
+    if (sigma.re == 0.0 && sigma.im == 0.0) {
       st->status = ST_BREAKDOWN;
       return;
     }
@@ -361,9 +407,7 @@ struct OpCocgB {
     const dcx a = ld_dcx(&st->alpha);
     malpha = mkc<R>((R)(-a.re), (R)(-a.im));
   }
-  __device__ void point(long long cell, int, int, int, const cx<R> W[3], double* acc) const {
-    R aW[3];
-    absW3<R>(W, aW);
+  __device__ void point(long long cell, int, int, int, const cx<R> W[3], const R aW[3], acc_t<R>* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const long long idx = c * N + cell;
@@ -380,12 +424,19 @@ struct OpCocgB {
   }
   __device__ void finish(const double* s) const {
     const dcx rho_new = {s[0], s[1]};
+    const double prev_pc = st->rr_pc;
     st->rr = s[2];
     st->rr_pc = s[3];
     st->rr_w2 = s[4];
     st->iter += 1;
     const bool ok = dfinite(rho_new);
     st->pending = ok ? 1 : 0;
+    // a near-zero p^T W q shows up as a residual explosion: the step is discarded
+    if (ok && s[3] > 1e16 * prev_pc) {
+      st->pending = 0;
+      st->status = ST_BREAKDOWN;
+      return;
+    }
     check_progress(st, monitored_rr(st), ok);
     if (st->status != ST_RUNNING) {
       st->rho = rho_new;
@@ -421,7 +472,7 @@ struct OpCocgFinal {
     alpha = from_d<R>(ld_dcx(&st->alpha));
     upd = __ldcg(&st->pending) != 0;
   }
-  __device__ void point(long long cell, int, int, int, const cx<R>*, double*) const {
+  __device__ void point(long long cell, int, int, int, const cx<R>*, const R*, acc_t<R>*) const {
     if (!upd) return;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -433,33 +484,15 @@ struct OpCocgFinal {
 };
 
 // ------------------------------------------------------------------ BiCGSTAB
-// Shadow vector: a fixed pseudo-random complex vector derived from the element
-// index (splitmix64), so it costs no memory traffic.
-__device__ __forceinline__ dcx shadow_d(long long idx, unsigned long long seed) {
-  unsigned long long z = (unsigned long long)idx * 0x9e3779b97f4a7c15ull + seed;
-  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
-  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
-  z ^= z >> 31;
-  const double a = (double)(unsigned)(z & 0xffffffffu) * (1.0 / 4294967296.0) - 0.5;
-  const double b = (double)(unsigned)(z >> 32) * (1.0 / 4294967296.0) - 0.5;
-  return {a, b};
-}
-template <typename R>
-__device__ __forceinline__ cx<R> shadow(long long idx, unsigned long long seed) {
-  dcx d = shadow_d(idx, seed);
-  return mkc<R>((R)d.re, (R)d.im);
-}
-// conj(a) * b accumulated in FP64
-template <typename R>
-__device__ __forceinline__ void acc_cdot(double* acc, cx<R> a, cx<R> b) {
-  acc[0] += (double)a.re * (double)b.re + (double)a.im * (double)b.im;
-  acc[1] += (double)a.re * (double)b.im - (double)a.im * (double)b.re;
-}
-
+// BiCGSTAB vectors (ping-pong pairs selected by iteration parity with ternaries, so
+// no runtime-indexed array forces the op into local memory).
 struct BsBufs {
-  void* R[2];
-  void* V[2];
-  void* P[2];
+  void* R0;
+  void* R1;
+  void* V0;
+  void* V1;
+  void* P0;
+  void* P1;
   void* T;
   void* x;
 };
@@ -469,7 +502,7 @@ struct BsBufs {
 //   x += alpha p_old + omega s ; v = A0 p ; sigma = (rh, v) ; |r|^2
 template <typename R>
 struct OpBsP {
-  static constexpr int NRED = 3;
+  static constexpr int NB = 4, NS = 2, NRED = 3;
   static constexpr bool NEEDS_W = false;
   BsBufs B;
   long long N;
@@ -485,55 +518,73 @@ struct OpBsP {
   cx<R>* x;
   cx<R> alpha, omega, beta, malpha, momega;
   bool upd;
+  struct Pre {
+    cx<R> x[3];
+  };
   __device__ bool skip() const { return ld_status(st) != ST_RUNNING; }
   __device__ void prepare() {
-    const int k = __ldcg(&st->iter);
-    const int o = k & 1, n = o ^ 1;
-    ro = (const cx<R>*)B.R[o];
-    vo = (const cx<R>*)B.V[o];
-    po = (const cx<R>*)B.P[o];
-    rn = (cx<R>*)B.R[n];
-    vn = (cx<R>*)B.V[n];
-    pn = (cx<R>*)B.P[n];
+    const bool odd = (__ldcg(&st->iter) & 1) != 0;
+    ro = (const cx<R>*)(odd ? B.R1 : B.R0);
+    vo = (const cx<R>*)(odd ? B.V1 : B.V0);
+    po = (const cx<R>*)(odd ? B.P1 : B.P0);
+    rn = (cx<R>*)(odd ? B.R0 : B.R1);
+    vn = (cx<R>*)(odd ? B.V0 : B.V1);
+    pn = (cx<R>*)(odd ? B.P0 : B.P1);
     t = (const cx<R>*)B.T;
     x = (cx<R>*)B.x;
     upd = __ldcg(&st->pending) != 0;
     if (upd) {
       alpha = from_d<R>(ld_dcx(&st->alpha));
       omega = from_d<R>(ld_dcx(&st->omega));
+      beta = from_d<R>(ld_dcx(&st->beta));
     } else {
       alpha = czero<R>();
       omega = czero<R>();
+      beta = czero<R>();
     }
-    beta = upd ? from_d<R>(ld_dcx(&st->beta)) : czero<R>();
     malpha = mkc<R>(-alpha.re, -alpha.im);
     momega = mkc<R>(-omega.re, -omega.im);
   }
-  __device__ cx<R> load(int, long long idx) const {
-    if (!upd) return ro[idx];
-    const cx<R> v = vo[idx];
-    const cx<R> s = caxpy(malpha, v, ro[idx]);
-    const cx<R> r = caxpy(momega, t[idx], s);
-    return caxpy(beta, caxpy(momega, v, po[idx]), r);
+  // the first pass (no owed update) only reads r: the other buffers are not initialised
+  __device__ const cx<R>* box_src(int bi) const {
+    if (!upd && bi > 0) return nullptr;
+    return bi == 0 ? ro : (bi == 1 ? vo : (bi == 2 ? t : po));
   }
-  __device__ void own(long long cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R>*,
-                      double* acc) const {
+  __device__ void pre(long long cell, Pre& p) const {
+    if (!upd) return;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) p.x[c] = x[c * N + cell];
+  }
+  // v = [r_old, v_old, t, p_old]
+  __device__ cx<R> make_u(const cx<R>* v, long long, int) const {
+    if (!upd) return v[0];
+    const cx<R> s = caxpy(malpha, v[1], v[0]);
+    const cx<R> r = caxpy(momega, v[2], s);
+    return caxpy(beta, caxpy(momega, v[1], v[3]), r);
+  }
+  // stash: r_new and the owed x update alpha p_old + omega s
+  __device__ void stash(const cx<R>* v, long long, int, cx<R>* out) const {
+    if (!upd) {
+      out[0] = v[0];
+      out[1] = czero<R>();
+      return;
+    }
+    const cx<R> s = caxpy(malpha, v[1], v[0]);
+    out[0] = caxpy(momega, v[2], s);
+    out[1] = caxpy(omega, s, alpha * v[3]);
+  }
+  __device__ void own(long long cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R>*, const R*,
+                      const cx<R>* sv, const Pre& pr, acc_t<R>* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const long long idx = c * N + cell;
-      cx<R> r;
-      if (upd) {
-        const cx<R> s = caxpy(malpha, vo[idx], ro[idx]);
-        r = caxpy(momega, t[idx], s);
-        x[idx] = caxpy(omega, s, caxpy(alpha, po[idx], x[idx]));
-      } else {
-        r = ro[idx];
-      }
+      const cx<R> r = sv[c * 2 + 0];
+      if (upd) x[idx] = pr.x[c] + sv[c * 2 + 1];
       rn[idx] = r;
       pn[idx] = u[c];
       vn[idx] = y[c];
       acc_cdot<R>(acc, shadow<R>(idx, seed), y[c]);
-      acc[2] += (double)cabs2(r);
+      acc[2] += cabs2(r);
     }
   }
   __device__ void finish(const double* s) const {
@@ -556,7 +607,7 @@ struct OpBsP {
 // S pass: s = r - alpha v ; t = A0 s ; (t,s), |t|^2, (rh,t), |s|^2 ; omega, rho, beta
 template <typename R>
 struct OpBsS {
-  static constexpr int NRED = 6;
+  static constexpr int NB = 2, NS = 0, NRED = 6;
   static constexpr bool NEEDS_W = false;
   BsBufs B;
   long long N;
@@ -566,27 +617,30 @@ struct OpBsS {
   const cx<R>* v;
   cx<R>* t;
   cx<R> malpha;
+  struct Pre {};
   __device__ bool skip() const { return ld_status(st) != ST_RUNNING; }
   __device__ void prepare() {
-    const int k = __ldcg(&st->iter);
-    const int n = (k & 1) ^ 1;
-    r = (const cx<R>*)B.R[n];
-    v = (const cx<R>*)B.V[n];
+    const bool odd = (__ldcg(&st->iter) & 1) != 0;
+    r = (const cx<R>*)(odd ? B.R0 : B.R1);
+    v = (const cx<R>*)(odd ? B.V0 : B.V1);
     t = (cx<R>*)B.T;
     const dcx a = ld_dcx(&st->alpha);
     malpha = mkc<R>((R)(-a.re), (R)(-a.im));
   }
-  __device__ cx<R> load(int, long long idx) const { return caxpy(malpha, v[idx], r[idx]); }
-  __device__ void own(long long cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R>*,
-                      double* acc) const {
+  __device__ const cx<R>* box_src(int bi) const { return bi == 0 ? r : v; }
+  __device__ void pre(long long, Pre&) const {}
+  __device__ cx<R> make_u(const cx<R>* vv, long long, int) const { return caxpy(malpha, vv[1], vv[0]); }
+  __device__ void stash(const cx<R>*, long long, int, cx<R>*) const {}
+  __device__ void own(long long cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R>*, const R*,
+                      const cx<R>*, const Pre&, acc_t<R>* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const long long idx = c * N + cell;
       t[idx] = y[c];
       acc_cdot<R>(acc, y[c], u[c]);                       // (t, s)
-      acc[2] += (double)cabs2(y[c]);                      // |t|^2
+      acc[2] += cabs2(y[c]);                              // |t|^2
       acc_cdot<R>(acc + 3, shadow<R>(idx, seed), y[c]);   // (rh, t)
-      acc[5] += (double)cabs2(u[c]);                      // |s|^2
+      acc[5] += cabs2(u[c]);                              // |s|^2
     }
   }
   __device__ void finish(const double* s) const {
@@ -630,7 +684,7 @@ struct OpBsS {
 // BiCGSTAB start: r = b - A0 x0 (x0 may be zero) ; rho = (rh, r) ; |r|^2 ; status.
 template <typename R>
 struct OpBsInit {
-  static constexpr int NRED = 3;
+  static constexpr int NB = 1, NS = 0, NRED = 3;
   static constexpr bool NEEDS_W = false;
   const cx<R>* b;
   const cx<R>* x;
@@ -638,15 +692,24 @@ struct OpBsInit {
   long long N;
   unsigned long long seed;
   KState* st;
+  struct Pre {
+    cx<R> b[3];
+  };
   __device__ bool skip() const { return false; }
   __device__ void prepare() {}
-  __device__ cx<R> load(int, long long idx) const { return x ? x[idx] : czero<R>(); }
-  __device__ void own(long long cell, int, int, int, const cx<R>*, const cx<R> y[3], const cx<R>*,
-                      double* acc) const {
+  __device__ const cx<R>* box_src(int) const { return x; }
+  __device__ void pre(long long cell, Pre& p) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) p.b[c] = b[c * N + cell];
+  }
+  __device__ cx<R> make_u(const cx<R>* v, long long, int) const { return v[0]; }
+  __device__ void stash(const cx<R>*, long long, int, cx<R>*) const {}
+  __device__ void own(long long cell, int, int, int, const cx<R>*, const cx<R> y[3], const cx<R>*, const R*,
+                      const cx<R>*, const Pre& pr, acc_t<R>* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const long long idx = c * N + cell;
-      const cx<R> rv = b[idx] - y[c];
+      const cx<R> rv = pr.b[c] - y[c];
       r[idx] = rv;
       acc_cdot<R>(acc, shadow<R>(idx, seed), rv);
       acc[2] += (double)cabs2(rv);
@@ -680,18 +743,17 @@ struct OpBsFinal {
   bool upd;
   __device__ bool skip() const { return false; }
   __device__ void prepare() {
-    const int k = __ldcg(&st->iter);
-    const int n = k & 1;
-    r = (const cx<R>*)B.R[n];
-    v = (const cx<R>*)B.V[n];
-    p = (const cx<R>*)B.P[n];
+    const bool odd = (__ldcg(&st->iter) & 1) != 0;
+    r = (const cx<R>*)(odd ? B.R1 : B.R0);
+    v = (const cx<R>*)(odd ? B.V1 : B.V0);
+    p = (const cx<R>*)(odd ? B.P1 : B.P0);
     x = (cx<R>*)B.x;
     upd = __ldcg(&st->pending) != 0;
     alpha = from_d<R>(ld_dcx(&st->alpha));
     omega = from_d<R>(ld_dcx(&st->omega));
     malpha = mkc<R>(-alpha.re, -alpha.im);
   }
-  __device__ void point(long long cell, int, int, int, const cx<R>*, double*) const {
+  __device__ void point(long long cell, int, int, int, const cx<R>*, const R*, acc_t<R>*) const {
     if (!upd) return;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -709,7 +771,7 @@ struct OpBsFinal {
 // (rh, r32) and |r32|^2 (the inner BiCGSTAB's starting rho and norm).
 template <typename RI>
 struct OpRefine {
-  static constexpr int NRED = 6;
+  static constexpr int NB = 1, NS = 0, NRED = 6;
   static constexpr bool NEEDS_W = true;
   const cx<double>* E_old;
   const cx<RI>* d;
@@ -720,25 +782,32 @@ struct OpRefine {
   long long N;
   unsigned long long seed;
   KState* st;
+  struct Pre {
+    cx<double> b[3];
+  };
   __device__ bool skip() const { return false; }
   __device__ void prepare() {}
-  __device__ cx<double> load(int, long long idx) const {
-    cx<double> e = E_old[idx];
+  __device__ const cx<double>* box_src(int) const { return E_old; }
+  __device__ void pre(long long cell, Pre& p) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) p.b[c] = b[c * N + cell];
+  }
+  __device__ cx<double> make_u(const cx<double>* v, long long idx, int) const {
+    cx<double> e = v[0];
     if (d) {
       const cx<RI> dv = d[idx];
       e = caxpy(mkc<double>(scale, 0.0), mkc<double>((double)dv.re, (double)dv.im), e);
     }
     return e;
   }
+  __device__ void stash(const cx<double>*, long long, int, cx<double>*) const {}
   __device__ void own(long long cell, int, int, int, const cx<double> u[3], const cx<double> y[3],
-                      const cx<double> W[3], double* acc) const {
-    double aW[3];
-    absW3<double>(W, aW);
+                      const cx<double>*, const double aW[3], const cx<double>*, const Pre& pr, double* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const long long idx = c * N + cell;
       E_new[idx] = u[c];
-      const cx<double> rv = b[idx] - y[c];
+      const cx<double> rv = pr.b[c] - y[c];
       const cx<RI> r1 = mkc<RI>((RI)(rscale * rv.re), (RI)(rscale * rv.im));
       rin[idx] = r1;
       const double r2 = cabs2(rv);
@@ -765,7 +834,7 @@ struct OpRefine {
 // matching weighted |b0|^2: the true and the symmetrised-system residuals.
 template <typename R>
 struct OpResidual {
-  static constexpr int NRED = 4;
+  static constexpr int NB = 1, NS = 0, NRED = 4;
   static constexpr bool NEEDS_W = true;
   const cx<R>* E;
   const cx<R>* J;
@@ -773,8 +842,16 @@ struct OpResidual {
   int adjoint;
   Geo<R> g;
   double* out;  // 4 doubles
+  struct Pre {
+    cx<R> j[3];
+  };
   __device__ bool skip() const { return false; }
   __device__ void prepare() {}
+  __device__ const cx<R>* box_src(int) const { return E; }
+  __device__ void pre(long long cell, Pre& p) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) p.j[c] = J[c * g.N + cell];
+  }
   __device__ cx<R> w_at(int c, long long idx) const {
     const long long cell = idx - c * g.N;
     const long long YZ = (long long)g.Y * g.Z;
@@ -785,8 +862,8 @@ struct OpResidual {
     if (c == 1) return g.dxh[0][i] * g.dxe[1][j] * g.dxh[2][k];
     return g.dxh[0][i] * g.dxh[1][j] * g.dxe[2][k];
   }
-  __device__ cx<R> load(int c, long long idx) const {
-    cx<R> e = E[idx];
+  __device__ cx<R> make_u(const cx<R>* v, long long idx, int c) const {
+    cx<R> e = v[0];
     if (adjoint) {
       const cx<R> w = w_at(c, idx);
       const R d = cabs2(w);
@@ -794,14 +871,12 @@ struct OpResidual {
     }
     return e;
   }
-  __device__ void own(long long cell, int, int, int, const cx<R>*, const cx<R> y[3], const cx<R> W[3],
-                      double* acc) const {
-    R aW[3];
-    absW3<R>(W, aW);
+  __device__ void stash(const cx<R>*, long long, int, cx<R>*) const {}
+  __device__ void own(long long, int, int, int, const cx<R>*, const cx<R> y[3], const cx<R> W[3],
+                      const R aW[3], const cx<R>*, const Pre& pr, acc_t<R>* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const long long idx = c * g.N + cell;
-      const cx<R> j = J[idx];
+      const cx<R> j = pr.j[c];
       const cx<R> b0 = mkc<R>((R)(om_im * j.re + om_re * j.im), (R)(om_im * j.im - om_re * j.re));
       const cx<R> ay = adjoint ? cconj(W[c] * y[c]) : y[c];
       const cx<R> rv = b0 - ay;
@@ -830,7 +905,7 @@ struct OpCopy {
   long long N;
   __device__ bool skip() const { return false; }
   __device__ void prepare() {}
-  __device__ void point(long long cell, int, int, int, const void*, double*) const {
+  __device__ void point(long long cell, int, int, int, const void*, const void*, acc_t<RD>*) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const long long idx = c * N + cell;
