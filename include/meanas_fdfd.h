@@ -159,6 +159,13 @@ int fdfd_residual_workspace_bytes(const fdfd_plan* plan, size_t* bytes);
 int fdfd_residual(fdfd_plan* plan, const void* E, const void* J, double out[4], void* ws,
                   size_t ws_bytes, void* stream);
 
+/* dL/d(epsilon) from the forward field E and the adjoint field E_adj
+ * (fdfd_solve with adjoint = 1 and J_adj = dL/dE* / (-i omega), torch's convention
+ * grad = 2 dL/dE*): grad[i] = Re(omega^2 conj(E_adj[i]) E[i]), zero on PEC components.
+ * No counterpart function in the reference, which assembles this from generic() and
+ * generic(adjoint=True) (meanas/fdfd/solvers.py:119-137); grad: float64[3N]. */
+int fdfd_eps_gradient(fdfd_plan* plan, const void* E, const void* E_adj, double* grad, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -88,6 +88,7 @@ EXPORTS = {
     'fdfd_residual_workspace_bytes': (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     'fdfd_residual': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_void_p,
                                 C.c_size_t, C.c_void_p]),
+    'fdfd_eps_gradient': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 _lib: C.CDLL | None = None

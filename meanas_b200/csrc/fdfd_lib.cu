@@ -920,3 +920,12 @@ extern "C" int fdfd_solve(fdfd_plan* P, const fdfd_solve_opts* o, const void* J,
   P->profiling = false;
   return c.status == ST_CONVERGED ? 0 : c.status;
 }
+
+// ------------------------------------------------------------------ gradient
+extern "C" int fdfd_eps_gradient(fdfd_plan* P, const void* E, const void* E_adj, double* grad, void* stream) {
+  if (!P || !E || !E_adj || !grad) return set_err(FDFD_ERR_ARG, "fdfd_eps_gradient: NULL argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  P->launches = 0;
+  OpEpsGrad<double> op{(const cx<double>*)E, (const cx<double>*)E_adj, grad, P->g64.w2, P->g64.mask, P->N};
+  return launch_point<double>(P, P->g64, 0, op, RedBuf{nullptr, nullptr}, s);
+}

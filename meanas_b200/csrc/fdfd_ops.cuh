@@ -895,6 +895,34 @@ struct OpResidual {
   }
 };
 
+// dL/deps from a forward field E and the adjoint field E_adj (A0^H E_adj = b_adj):
+// grad = Re(omega^2 conj(E_adj) E) on non-PEC components, 0 on PEC ones.  With
+// lambda = conj(E_adj) solving A0^T lambda = conj(dL/dE), this is the derivative of
+// L through A0 = pe (... - omega^2 eps) pe (meanas/fdfd/operators.py:95).
+template <typename R>
+struct OpEpsGrad {
+  static constexpr int NRED = 0;
+  static constexpr bool NEEDS_W = false;
+  const cx<R>* E;
+  const cx<R>* Ea;
+  R* grad;
+  cx<R> w2;
+  const uint8_t* mask;
+  long long N;
+  __device__ bool skip() const { return false; }
+  __device__ void prepare() {}
+  __device__ void point(long long cell, int, int, int, const cx<R>*, const R*, acc_t<R>*) const {
+    const uint8_t m = mask ? mask[cell] : (uint8_t)0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long idx = c * N + cell;
+      const cx<R> v = w2 * (cconj(Ea[idx]) * E[idx]);
+      grad[idx] = (m & (1u << c)) ? R(0) : v.re;
+    }
+  }
+  __device__ void finish(const double*) const {}
+};
+
 // Copy / convert / zero helpers (pointwise over the 3 components of each cell).
 template <typename RS, typename RD>
 struct OpCopy {

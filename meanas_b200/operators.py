@@ -180,6 +180,16 @@ class GridOperator:
         r, rpc, b, bpc = list(out)
         return dict(abs=r, rel=r / b if b else r, abs_pc=rpc, rel_pc=rpc / bpc if bpc else rpc, b=b, b_pc=bpc)
 
+    def eps_gradient(self, E: torch.Tensor, E_adj: torch.Tensor) -> torch.Tensor:
+        """``Re(omega^2 conj(E_adj) E)`` per component (zero on PEC): dL/deps given the adjoint field."""
+        Et = as_device(E, torch.complex128, self.device, self.n, 'E')
+        Ea = as_device(E_adj, torch.complex128, self.device, self.n, 'E_adj')
+        g = torch.empty(self.n, dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.fdfd_eps_gradient(self.plan, Et.data_ptr(), Ea.data_ptr(), g.data_ptr(),
+                                                  _stream_handle()))
+        return g
+
     # ------------------------------------------------------------------ solve
     def solve_opts(self, *, method: str = 'cocg', rtol: float = 1e-8, atol: float = 0.0,
                    maxiter: int | None = None, criterion: str = 'true', adjoint: bool = False,
