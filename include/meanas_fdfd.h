@@ -166,6 +166,17 @@ int fdfd_residual(fdfd_plan* plan, const void* E, const void* J, double out[4], 
  * generic(adjoint=True) (meanas/fdfd/solvers.py:119-137); grad: float64[3N]. */
 int fdfd_eps_gradient(fdfd_plan* plan, const void* E, const void* E_adj, double* grad, void* stream);
 
+/* fdfd_residual without a workspace, for callers that cannot allocate device memory
+ * (an exhausted or frozen allocator, or a host program that owns every device buffer
+ * and can pass only inputs and outputs).  No counterpart in the reference.
+ * The reduction scratch is a fixed 1 MiB array inside the library, held by every
+ * device that loads it until exit; grids needing more than 32752 CTAs are rejected
+ * with FDFD_ERR_ARG.  The first call on a device looks up that array's device
+ * address; make it before any stream capture.  All calls share the array: calls
+ * whose work overlaps on the GPU (other streams, other threads) race on it.
+ * Allocates nothing; same results as fdfd_residual. */
+int fdfd_residual_static(fdfd_plan* plan, const void* E, const void* J, double out[4], void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -89,6 +89,7 @@ EXPORTS = {
     'fdfd_residual': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_void_p,
                                 C.c_size_t, C.c_void_p]),
     'fdfd_eps_gradient': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    'fdfd_residual_static': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_void_p]),
 }
 
 _lib: C.CDLL | None = None

@@ -9,6 +9,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -928,4 +929,66 @@ extern "C" int fdfd_eps_gradient(fdfd_plan* P, const void* E, const void* E_adj,
   P->launches = 0;
   OpEpsGrad<double> op{(const cx<double>*)E, (const cx<double>*)E_adj, grad, P->g64.w2, P->g64.mask, P->N};
   return launch_point<double>(P, P->g64, 0, op, RedBuf{nullptr, nullptr}, s);
+}
+
+// ------------------------------------------------------------------ allocation-free residual
+// For callers that cannot allocate device memory at all (for example code running
+// under an allocator that is already exhausted or frozen, or a host application
+// that owns every device buffer and hands out only inputs and outputs): the FP64
+// residual check with its reduction scratch in this fixed array instead of a
+// caller-provided workspace.  Every device that loads the library keeps these
+// bytes until the process exits.
+constexpr size_t STATIC_SCRATCH_BYTES = (size_t)1 << 20;  // 1 MiB per device
+static __device__ __align__(256) unsigned char g_static_scratch[STATIC_SCRATCH_BYTES];
+
+constexpr int STATIC_MAX_DEVICES = 64;
+static std::mutex g_static_mutex;
+static void* g_static_addr[STATIC_MAX_DEVICES];
+
+// Device address of g_static_scratch on the current device (looked up once per device:
+// in host code the array's name is only a host-side stand-in).
+static int static_scratch_address(void** out) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= STATIC_MAX_DEVICES)
+    return set_err(FDFD_ERR_ARG, "fdfd_residual_static: device %d beyond %d", dev, STATIC_MAX_DEVICES);
+  std::lock_guard<std::mutex> lock(g_static_mutex);
+  if (!g_static_addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess)
+      return set_err(FDFD_ERR_CUDA, "fdfd_residual_static: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+    g_static_addr[dev] = p;
+  }
+  *out = g_static_addr[dev];
+  return 0;
+}
+
+extern "C" int fdfd_residual_static(fdfd_plan* P, const void* E, const void* J, double out[4], void* stream) {
+  if (!P || !E || !J || !out) return set_err(FDFD_ERR_ARG, "fdfd_residual_static: NULL argument");
+  // scratch layout: [0, 256) ticket, [256, 512) the four sums, [512, ...) per-CTA partials
+  const Tiling t = make_tiling(P, 0);
+  const size_t need = 512 + (size_t)t.nblocks * OpResidual<double>::NRED * sizeof(double);
+  if (need > STATIC_SCRATCH_BYTES)
+    return set_err(FDFD_ERR_ARG,
+                   "fdfd_residual_static: the grid needs %lld CTAs (%zu scratch bytes); the fixed scratch holds "
+                   "%zu bytes (at most %zu CTAs) -- use fdfd_residual with a workspace",
+                   (long long)t.nblocks, need, STATIC_SCRATCH_BYTES,
+                   (STATIC_SCRATCH_BYTES - 512) / (OpResidual<double>::NRED * sizeof(double)));
+  void* base = nullptr;
+  TRY(static_scratch_address(&base));
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned char* b = (unsigned char*)base;
+  unsigned int* ticket = (unsigned int*)b;
+  double* d_out = (double*)(b + 256);
+  RedBuf rb{(double*)(b + 512), ticket};
+  P->launches = 0;
+  // the ticket must start at zero; the partials and sums are fully rewritten
+  CK(cudaMemsetAsync(ticket, 0, sizeof(unsigned int), s));
+  TRY(residual_into(P, E, J, 0, d_out, rb, s));
+  CK(cudaMemcpyAsync(P->h_state, d_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  const double* h = (const double*)P->h_state;
+  for (int i = 0; i < 4; ++i) out[i] = std::sqrt(h[i]);
+  return 0;
 }
