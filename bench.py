@@ -42,11 +42,20 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = 'FDFD solves/s at FP64 residual 1e-8, mixed vs FP64 GPU; p50/p99 latency'
-WORKLOAD = dict(workload='aniso_blocks 160x160x128, 12-cell SC-PML, omega=2pi/24, '
-                         'diag-anisotropic eps blocks {1,2.1,12.1}, Gaussian Jy plane z=20',
-                shape=[160, 160, 128], unknowns=3 * 160 * 160 * 128, rtol=1e-8,
+WORKLOADS = {
+    'aniso_blocks': 'aniso_blocks 160x160x128, 12-cell SC-PML, omega=2pi/24, '
+                    'diag-anisotropic eps blocks {1,2.1,12.1}, Gaussian Jy plane z=20',
+    'dipole_core': 'dipole_core 48^3, 10-cell SC-PML, omega=2pi/30, eps=12.1 core, unit Jz dipole',
+    'masked_large': 'masked_large 320x320x200, 16-cell SC-PML, omega=2pi/20, eps in [1,12.1], '
+                    'mu in [1,1.5], PEC 5% / PMC 2% slabs, 3 dipoles',
+}
+
+
+def workload_config(name: str, p) -> dict:
+    return dict(workload=WORKLOADS[name], shape=list(p.shape), unknowns=p.n_unknowns, rtol=1e-8,
                 criterion='true FP64 residual ||b0-A0 E||/||b0||',
-                l2='inputs and per-iteration vectors larger than L2 (no flush)')
+                l2=('inputs and per-iteration vectors larger than L2 (no flush)' if p.n_cells * 456 > 126e6
+                    else 'working set fits in L2 (small reference case)'))
 RTOL = 1e-8
 # Algorithmic bytes per cell of each iteration kernel ("Kernels"):
 #   COCG stencil pass (c128): read r, p_old, x, eps; write p, x, q   = 6*48 + 24 = 312
@@ -168,9 +177,9 @@ def run_ours(args) -> dict | None:
 
     rank, world, local = dist_setup(args.gpus)
     dev = torch.device('cuda', torch.cuda.current_device())
-    p = workloads.aniso_blocks()
+    p = workloads.BY_NAME[args.workload]()
     ncell = p.n_cells
-    op = GridOperator(p.omega, p.dxes, p.epsilon, device=dev, fp32=True)
+    op = GridOperator(p.omega, p.dxes, p.epsilon, p.mu, p.pec, p.pmc, device=dev, fp32=True)
     J = torch.as_tensor(p.J, device=dev)
     stream = torch.cuda.current_stream()
 
@@ -221,19 +230,21 @@ def run_ours(args) -> dict | None:
         epsh = torch.from_numpy(p.epsilon).pin_memory()
         best = max(out, key=lambda m: out[m]['solves_per_s'])
         prec = 'mixed' if best == 'mixed' else 'fp64'
+        extra = dict(mu=p.mu, pec=p.pec, pmc=p.pmc)
         generic(p.omega, p.dxes, Jh, epsh, precision=prec, criterion='true',
-                matrix_solver_opts=dict(rtol=RTOL), device=dev)
+                matrix_solver_opts=dict(rtol=RTOL), device=dev, **extra)
         barrier_sync(world)
         t = time.perf_counter()
         for _ in range(args.e2e_steps):
             E = generic(p.omega, p.dxes, Jh, epsh, precision=prec, criterion='true',
-                        matrix_solver_opts=dict(rtol=RTOL), device=dev)
+                        matrix_solver_opts=dict(rtol=RTOL), device=dev, **extra)
         barrier_sync(world)
         el = max_over_ranks(time.perf_counter() - t, world)
         assert E.shape == (p.n_unknowns,)
         table_bytes = sum(16 * 2 * numpy.size(d) for g in p.dxes for d in g)
+        opt_bytes = sum(8 * a.size for a in (p.mu, p.pec, p.pmc) if a is not None)
         e2e = dict(value=world * args.e2e_steps / el, unit='solves/s', method=prec,
-                   h2d_bytes_per_step=int(Jh.numel() * 16 + epsh.numel() * 8 + table_bytes),
+                   h2d_bytes_per_step=int(Jh.numel() * 16 + epsh.numel() * 8 + table_bytes + opt_bytes),
                    d2h_bytes_per_step=int(p.n_unknowns * 16))
 
     if rank != 0:
@@ -245,7 +256,11 @@ def run_ours(args) -> dict | None:
     kinds = [0, 1] if best == 'cocg' else [2, 3]
     dom = max(kinds, key=lambda k: b['kernel_ms'][k])
     avg_ms = b['kernel_ms'][dom] / max(1, b['kernel_count'][dom])
-    alg = KERNEL_BYTES_PER_CELL[dom] * ncell
+    extra_bytes = 0  # mu^-1 (3 reals) and the mask byte read by the stencil passes
+    if dom in (0, 2, 3):
+        real = 8 if dom == 0 else 4
+        extra_bytes = (3 * real if p.mu is not None else 0) + (1 if (p.pec is not None or p.pmc is not None) else 0)
+    alg = (KERNEL_BYTES_PER_CELL[dom] + extra_bytes) * ncell
     achieved = alg / (avg_ms / 1e3) / 1e9
     traffic = profile_traffic(KERNEL_NAMES[dom])
     share = b['kernel_ms'][dom] / (b['ms_per_step'] * args.steps)
@@ -256,7 +271,7 @@ def run_ours(args) -> dict | None:
         'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
         'dtype': 'c64 inner + c128 refinement' if best == 'mixed' else 'c128',
         'data': 'synthetic (seeded)',
-        'config': dict(WORKLOAD, method=best, parallelism=f'replicas x{world}'),
+        'config': dict(workload_config(args.workload, p), method=best, parallelism=f'replicas x{world}'),
         'p50_ms': round(b['p50_ms'], 3), 'p99_ms': round(b['p99_ms'], 3),
         'mixed': ({k: v for k, v in out['mixed'].items() if k not in ('kernel_ms', 'kernel_count')}
                   if 'mixed' in out else None),
@@ -280,13 +295,14 @@ def run_ours(args) -> dict | None:
 
 
 def cpu_baseline(p, sample_iters: int, iters_full: int) -> dict:
+    # (mu, PEC and PMC enter the CSR assembly like the reference's e_full)
     """Oracle port of the reference path timed on the host: assembly + `sample_iters`
     scipy QMR iterations, extrapolated to `iters_full` iterations per solve."""
     import scipy.sparse.linalg
     from scipy import sparse
     from oracle import fdfd_oracle as O
     t0 = time.perf_counter()
-    A0 = O.e_full_csr(p.omega, p.dxes, p.epsilon)
+    A0 = O.e_full_csr(p.omega, p.dxes, p.epsilon, p.mu, p.pec, p.pmc)
     pl = O.precond_pl(p.dxes)
     A = (sparse.diags_array(pl) @ A0 @ sparse.diags_array(1 / pl)).tocsr()
     b = pl * (-1j * p.omega * p.J)
@@ -297,7 +313,7 @@ def cpu_baseline(p, sample_iters: int, iters_full: int) -> dict:
     t_solve = (t1 - t0) + iters_full * t_iter
     return {'value': round(1.0 / t_solve, 6), 'unit': 'solves/s', 'cores': 1, 'kind': 'port',
             'sample': f'CSR assembly ({t1 - t0:.1f} s) + {sample_iters} scipy QMR iterations '
-                      f'({t_iter * 1e3:.0f} ms each) on the full 160x160x128 system, extrapolated to '
+                      f'({t_iter * 1e3:.0f} ms each) on the full {"x".join(map(str, p.shape))} system, extrapolated to '
                       f'{iters_full} iterations (the GPU complex128 COCG count; the reference QMR took '
                       f'1189 vs COCG 1192 on the 48^3 case)',
             'seconds_per_solve': round(t_solve, 1)}
@@ -308,7 +324,7 @@ def run_reference(args) -> dict | None:
     if rank != 0:
         return None
     from meanas_b200 import workloads
-    p = workloads.aniso_blocks()
+    p = workloads.BY_NAME[args.workload]()
     samples = []
     iters_full = args.ref_iters
     for _ in range(args.warmup + args.steps):
@@ -318,7 +334,7 @@ def run_reference(args) -> dict | None:
     return {'metric': METRIC, 'value': v, 'unit': 'solves/s', 'n_gpus': args.gpus, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': 1e3 / v, 'higher_is_better': True, 'scaling': 'weak',
             'vs_baseline': None, 'dtype': 'c128', 'data': 'synthetic (seeded)', 'impl': 'reference',
-            'config': dict(WORKLOAD, method='scipy qmr (reference generic() algorithm, CPU)'),
+            'config': dict(workload_config(args.workload, p), method='scipy qmr (reference generic() algorithm, CPU)'),
             'cpu_baseline': {'value': v, 'unit': 'solves/s', 'cores': 1, 'kind': 'port',
                              'sample': timed[0]['sample']},
             'e2e': {'value': v, 'unit': 'solves/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
@@ -361,6 +377,52 @@ def kernel_mode(args) -> None:
               f'{per_cell * p.n_cells / (ms / 1e3) / 1e9:7.1f} GB/s algorithmic')
 
 
+def gradient_check(args) -> dict:
+    """dL/d(eps) on the 96x96x64 adjoint problem (L = sum |E|^2 over the plane x=76) by
+    torch.autograd (one forward + one adjoint GPU solve) against central finite differences
+    (h = 1e-4, FP64 solves to relative residual 1e-12) on `fd_cells` random design cells."""
+    import torch
+    from meanas_b200 import workloads
+    from meanas_b200.autograd import fdfd_solve
+    p = workloads.adjoint_design()
+    dev = torch.device('cuda', 0)
+    mon = torch.as_tensor(p.extra['monitor'], device=dev)
+    eps = torch.as_tensor(p.epsilon, device=dev).requires_grad_(True)
+    kw = dict(rtol=1e-12, criterion='true')
+
+    def loss(e):
+        E = fdfd_solve(e, p.J, p.omega, p.dxes, **kw)
+        return (E.abs() ** 2)[mon].sum()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    L = loss(eps)
+    L.backward()
+    torch.cuda.synchronize()
+    t_grad = time.perf_counter() - t0
+    g = eps.grad.cpu().numpy()
+    n = p.n_cells
+    cells = numpy.flatnonzero(p.extra['design_mask'].ravel())
+    rng = numpy.random.default_rng(0)
+    h = 1e-4
+    errs = []
+    with torch.no_grad():
+        for cell in rng.choice(cells, args.fd_cells, replace=False):
+            idx = [cell, n + cell, 2 * n + cell]
+            ep = eps.detach().clone()
+            em = eps.detach().clone()
+            ep[idx] += h
+            em[idx] -= h
+            fd = (loss(ep) - loss(em)).item() / (2 * h)
+            ad = float(g[idx].sum())
+            errs.append(abs(fd - ad) / max(abs(fd), 1e-300))
+    design_g = g[numpy.tile(p.extra['design_mask'].ravel(), 3)]
+    return {'metric': 'adjoint gradient dL/deps vs central finite differences', 'workload':
+            'adjoint_design 96x96x64, 10-cell SC-PML, omega=2pi/26, 40x40x8 design, L=sum|E|^2 at x=76',
+            'fd_cells': args.fd_cells, 'h': h, 'solve_rtol': 1e-12, 'max_rel_err': max(errs),
+            'median_rel_err': float(numpy.median(errs)), 'gradient_seconds': round(t_grad, 3),
+            'loss': L.item(), 'grad_norm_design': float(numpy.linalg.norm(design_g))}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -372,12 +434,19 @@ def main():
     ap.add_argument('--ref-iters', type=int, default=3000,
                     help='QMR iterations per full solve used to extrapolate the reference arm')
     ap.add_argument('--methods', default='mixed,cocg', help='GPU solvers to time (mixed, cocg)')
+    ap.add_argument('--workload', default='aniso_blocks', choices=sorted(WORKLOADS),
+                    help='problem (default: the 160x160x128 headline case)')
     ap.add_argument('--kernel-iters', type=int, default=0,
                     help='profiling mode: run this many iterations of each solver (no convergence, no JSON)')
     ap.add_argument('--shape', type=int, nargs=3, default=None, help='profiling mode grid shape')
+    ap.add_argument('--gradient-check', action='store_true', help='adjoint gradient vs finite differences')
+    ap.add_argument('--fd-cells', type=int, default=64)
     args = ap.parse_args()
     if args.kernel_iters > 0:
         return kernel_mode(args)
+    if args.gradient_check:
+        print(json.dumps(gradient_check(args)), flush=True)
+        return None
     res = run_reference(args) if args.impl == 'reference' else run_ours(args)
     if res is not None:
         print(json.dumps(res), flush=True)
