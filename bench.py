@@ -182,6 +182,7 @@ def run_ours(args) -> dict | None:
     op = GridOperator(p.omega, p.dxes, p.epsilon, p.mu, p.pec, p.pmc, device=dev, fp32=True)
     J = torch.as_tensor(p.J, device=dev)
     stream = torch.cuda.current_stream()
+    tuned = op.autotune(methods=tuple(args.methods.split(','))) if args.autotune else {}
 
     def timed(method: str, steps: int, warmup: int, profile: bool):
         kw = dict(method=method, rtol=RTOL, criterion='true', profile=profile)
@@ -285,6 +286,7 @@ def run_ours(args) -> dict | None:
                      'algorithmic_bytes_per_launch': alg, 'avg_launch_ms': round(avg_ms, 5),
                      'share_of_step': round(share, 3)},
         'gpu_launches': int(b['launches']),
+        'tiling': {k: {'xchunk': v[0], 'us_per_iteration': round(v[1], 1)} for k, v in tuned.items()},
         'clocks': clocks,
         'e2e': e2e,
     }
@@ -423,6 +425,45 @@ def gradient_check(args) -> dict:
             'loss': L.item(), 'grad_norm_design': float(numpy.linalg.norm(design_g))}
 
 
+def serving_run(args) -> dict:
+    """config[2]: a seeded Poisson stream of requests (sizes uniform over 128^2..1024^2 x1 and
+    32^3..128^3, lambda ~ U[16, 40] cells, random eps blocks, one dipole each), mixed precision
+    to a true FP64 residual of 1e-8, served with continuous batching."""
+    import torch
+    from meanas_b200 import serving
+    dev = torch.device('cuda', 0)
+    stream = serving.poisson_stream(args.serving, rate=args.rate, seed=0)
+    # warm each slot size (kernels, captured iteration graphs) with one request, untimed
+    warm = {}
+    for _, p in stream:
+        warm.setdefault(p.shape, p)
+    with serving.FDFDServer(dev, max_active=args.max_active, precision='mixed', rtol=RTOL) as srv:
+        for p in warm.values():
+            srv.submit(serving.Request(p.omega, p.dxes, p.J, p.epsilon)).result()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        results = serving.replay(srv, stream)
+        t1 = time.perf_counter()
+        stats = dict(srv.stats)
+    lat = numpy.array([r.latency for r in results]) * 1e3
+    ok = all(r.info.converged and r.info.residual <= RTOL for r in results)
+    by_size = {}
+    for (_, p), r in zip(stream, results):
+        by_size.setdefault('x'.join(map(str, p.shape)), []).append(r.latency * 1e3)
+    return {'metric': 'FDFD serving solves/s and p50/p99 latency (continuous batching)',
+            'value': round(len(results) / (t1 - t0), 3), 'unit': 'solves/s',
+            'requests': len(results), 'arrival_rate_per_s': args.rate,
+            'offered_seconds': round(stream[-1][0], 2), 'wall_seconds': round(t1 - t0, 2),
+            'p50_ms': round(float(numpy.percentile(lat, 50)), 1),
+            'p99_ms': round(float(numpy.percentile(lat, 99)), 1),
+            'all_converged_to_1e-8': ok, 'max_active': args.max_active, 'slots': stats,
+            'p50_ms_by_size': {k: round(float(numpy.median(v)), 1) for k, v in sorted(by_size.items())},
+            'iterations_by_size': {k: int(numpy.median([r.info.iterations for (_, p), r in zip(stream, results)
+                                                        if 'x'.join(map(str, p.shape)) == k]))
+                                   for k in sorted(by_size)},
+            'precision': 'c64 BiCGSTAB inner + c128 refinement', 'data': 'synthetic (seeded)'}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -434,18 +475,26 @@ def main():
     ap.add_argument('--ref-iters', type=int, default=3000,
                     help='QMR iterations per full solve used to extrapolate the reference arm')
     ap.add_argument('--methods', default='mixed,cocg', help='GPU solvers to time (mixed, cocg)')
+    ap.add_argument('--no-autotune', dest='autotune', action='store_false',
+                    help='keep the default tiling instead of timing x-chunk candidates first')
     ap.add_argument('--workload', default='aniso_blocks', choices=sorted(WORKLOADS),
                     help='problem (default: the 160x160x128 headline case)')
     ap.add_argument('--kernel-iters', type=int, default=0,
                     help='profiling mode: run this many iterations of each solver (no convergence, no JSON)')
     ap.add_argument('--shape', type=int, nargs=3, default=None, help='profiling mode grid shape')
     ap.add_argument('--gradient-check', action='store_true', help='adjoint gradient vs finite differences')
+    ap.add_argument('--serving', type=int, default=0, help='serving mode: replay this many requests')
+    ap.add_argument('--rate', type=float, default=50.0, help='serving: Poisson arrival rate (requests/s)')
+    ap.add_argument('--max-active', type=int, default=8, help='serving: solves in flight at once')
     ap.add_argument('--fd-cells', type=int, default=64)
     args = ap.parse_args()
     if args.kernel_iters > 0:
         return kernel_mode(args)
     if args.gradient_check:
         print(json.dumps(gradient_check(args)), flush=True)
+        return None
+    if args.serving > 0:
+        print(json.dumps(serving_run(args)), flush=True)
         return None
     res = run_reference(args) if args.impl == 'reference' else run_ours(args)
     if res is not None:

@@ -129,6 +129,13 @@ int fdfd_plan_workspace_bytes(const fdfd_grid_desc* desc, size_t* bytes);
 int fdfd_plan_create(const fdfd_grid_desc* desc, void* ws, size_t ws_bytes, void* stream,
                      fdfd_plan** out);
 
+/* Refill an existing plan from a new description of the same shape, flags and set of
+ * optional arrays (new omega, cell widths, epsilon, mu, masks), on `stream`.  The
+ * plan keeps its workspace and tiling, so iteration graphs captured for it stay valid
+ * when the array pointers are unchanged.  Used by the serving loop, whose slots
+ * serve request after request of one grid size (no counterpart in the reference). */
+int fdfd_plan_update(fdfd_plan* plan, const fdfd_grid_desc* desc, void* stream);
+
 /* Release the host-side plan object (the caller owns `ws`). */
 int fdfd_plan_destroy(fdfd_plan* plan);
 

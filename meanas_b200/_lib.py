@@ -79,6 +79,7 @@ EXPORTS = {
     'fdfd_last_error': (C.c_char_p, []),
     'fdfd_plan_workspace_bytes': (C.c_int, [C.POINTER(GridDesc), C.POINTER(C.c_size_t)]),
     'fdfd_plan_create': (C.c_int, [C.POINTER(GridDesc), C.c_void_p, C.c_size_t, C.c_void_p, C.POINTER(C.c_void_p)]),
+    'fdfd_plan_update': (C.c_int, [C.c_void_p, C.POINTER(GridDesc), C.c_void_p]),
     'fdfd_plan_destroy': (C.c_int, [C.c_void_p]),
     'fdfd_plan_set_xchunk': (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     'fdfd_apply': (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -101,7 +101,7 @@ struct Geo {
   const R* eps;          // 3N
   const R* muinv;        // 3N or null
   const uint8_t* mask;   // N or null
-  cx<R> w2;              // omega^2
+  const cx<R>* w2p;      // omega^2, in device memory (so captured graphs survive a new omega)
 };
 
 __device__ __forceinline__ int wrapi(int v, int n) {
@@ -284,6 +284,7 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
   if (op.skip()) return;
   Op o = op;
   o.prepare();
+  const cx<R> w2 = *g.w2p;
 
   const int tz = threadIdx.x, ty = threadIdx.y, tid = tz + ty * TZ;
   int b = blockIdx.x;
@@ -535,7 +536,7 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
       const uint8_t m = g.mask ? g.mask[cell] : (uint8_t)0;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        cx<R> v = y[c] - (e3[c] * g.w2) * u[c];
+        cx<R> v = y[c] - (e3[c] * w2) * u[c];
         if (m & (1u << c)) v = czero<R>();
         y[c] = v;
       }

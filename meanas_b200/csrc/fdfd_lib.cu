@@ -64,6 +64,11 @@ __global__ void k_recip_real(const double* src, double* dst64, float* dst32, lon
   }
 }
 
+__global__ void k_set_w2(cx<double>* w64, cx<float>* w32, double re, double im) {
+  *w64 = mkc<double>(re, im);
+  *w32 = mkc<float>((float)re, (float)im);
+}
+
 __global__ void k_to_f32(const double* src, float* dst, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     dst[i] = (float)src[i];
@@ -110,6 +115,9 @@ struct fdfd_plan {
   int X, Y, Z;
   long long N;
   int flags;
+  char* ws;                // plan workspace (caller's)
+  bool has_mu, has_mask;
+  cx<double> w2;           // omega^2 (host copy)
   double om_re, om_im;
   bool flat;
   bool has32;
@@ -224,12 +232,16 @@ static long long max_blocks(const fdfd_plan* P) {
 }
 
 // ------------------------------------------------------------------ launches
+static std::mutex g_smem_mutex;
+
 template <typename K>
 static void ensure_smem(K kern, size_t bytes) {
-  // only needed above the 48 KB default; remembered per kernel
+  // only needed above the 48 KB default; remembered per kernel (plans may run on
+  // several host threads at once)
   static std::vector<const void*> done;
   if (bytes <= 48 * 1024) return;
   const void* key = (const void*)kern;
+  std::lock_guard<std::mutex> lock(g_smem_mutex);
   if (std::find(done.begin(), done.end(), key) != done.end()) return;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   done.push_back(key);
@@ -283,7 +295,7 @@ extern "C" int fdfd_abi_version(void) { return FDFD_ABI_VERSION; }
 extern "C" const char* fdfd_last_error(void) { return g_err.c_str(); }
 
 struct PlanLayout {
-  size_t muinv64, muinv32, eps32, mask, tab64, tab32, total;
+  size_t consts, muinv64, muinv32, eps32, mask, tab64, tab32, total;
 };
 
 static int plan_layout(const fdfd_grid_desc* d, PlanLayout* L) {
@@ -294,6 +306,8 @@ static int plan_layout(const fdfd_grid_desc* d, PlanLayout* L) {
   const long long S = (long long)d->shape[0] + d->shape[1] + d->shape[2];
   const bool f32 = (d->flags & FDFD_GRID_FP32) != 0;
   size_t off = 0;
+  L->consts = off;  // omega^2 (complex128, complex64)
+  off += 256;
   L->muinv64 = off;
   if (d->mu) off += align256(3 * N * sizeof(double));
   L->muinv32 = off;
@@ -310,53 +324,9 @@ static int plan_layout(const fdfd_grid_desc* d, PlanLayout* L) {
   return 0;
 }
 
-extern "C" int fdfd_plan_workspace_bytes(const fdfd_grid_desc* desc, size_t* bytes) {
-  PlanLayout L;
-  TRY(plan_layout(desc, &L));
-  if (!bytes) return set_err(FDFD_ERR_ARG, "bytes is NULL");
-  *bytes = L.total;
-  return 0;
-}
-
-extern "C" int fdfd_plan_create(const fdfd_grid_desc* d, void* ws, size_t ws_bytes, void* stream,
-                                fdfd_plan** out) {
-  PlanLayout L;
-  TRY(plan_layout(d, &L));
-  if (!out) return set_err(FDFD_ERR_ARG, "out is NULL");
-  if (!d->epsilon) return set_err(FDFD_ERR_ARG, "epsilon is NULL");
-  for (int a = 0; a < 3; ++a)
-    if (!d->dxe[a] || !d->dxh[a]) return set_err(FDFD_ERR_ARG, "dxe/dxh[%d] is NULL", a);
-  if (ws_bytes < L.total || (L.total > 0 && !ws))
-    return set_err(FDFD_ERR_WORKSPACE, "plan workspace too small: %zu < %zu", ws_bytes, L.total);
-  if (((uintptr_t)ws & 255) != 0) return set_err(FDFD_ERR_ARG, "plan workspace must be 256-byte aligned");
-  cudaStream_t s = (cudaStream_t)stream;
-  fdfd_plan* P = new fdfd_plan();
-  P->X = d->shape[0];
-  P->Y = d->shape[1];
-  P->Z = d->shape[2];
-  P->N = (long long)P->X * P->Y * P->Z;
-  P->flags = d->flags;
-  P->om_re = d->omega[0];
-  P->om_im = d->omega[1];
-  P->flat = (P->Z == 1);
-  P->has32 = (d->flags & FDFD_GRID_FP32) != 0;
-  P->xc_override[0] = P->xc_override[1] = 0;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&P->nsm, cudaDevAttrMultiProcessorCount, dev);
-  if (P->nsm <= 0) P->nsm = 148;
-  auto cleanup = [&](int rc) {
-    delete P;
-    return rc;
-  };
-  if (cudaStreamCreateWithFlags(&P->cap, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&P->ev[0], cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&P->ev[1], cudaEventDisableTiming) != cudaSuccess ||
-      cudaMallocHost((void**)&P->h_poll, 8 * sizeof(int)) != cudaSuccess ||
-      cudaMallocHost((void**)&P->h_state, sizeof(KState)) != cudaSuccess)
-    return cleanup(set_err(FDFD_ERR_CUDA, "plan: stream/event/pinned allocation failed"));
-
-  char* base = (char*)ws;
+// (Re)compute everything the plan derives from a grid description into its workspace.
+static void plan_fill(fdfd_plan* P, const fdfd_grid_desc* d, const PlanLayout& L, cudaStream_t s) {
+  char* base = P->ws;
   const long long N = P->N;
   const int sh[3] = {P->X, P->Y, P->Z};
   // 1D tables: [dxe | dxh | idxe | idxh], each X+Y+Z long (axis-major)
@@ -421,17 +391,96 @@ extern "C" int fdfd_plan_create(const fdfd_grid_desc* d, void* ws, size_t ws_byt
   }
   P->g64.mask = mask;
   P->g32.mask = mask;
+  P->om_re = d->omega[0];
+  P->om_im = d->omega[1];
   const double w2re = P->om_re * P->om_re - P->om_im * P->om_im;
   const double w2im = 2.0 * P->om_re * P->om_im;
-  P->g64.w2 = mkc<double>(w2re, w2im);
-  P->g32.w2 = mkc<float>((float)w2re, (float)w2im);
+  P->w2 = mkc<double>(w2re, w2im);
+  cx<double>* c64p = (cx<double>*)(base + L.consts);
+  cx<float>* c32p = (cx<float>*)(base + L.consts + 64);
+  k_set_w2<<<1, 1, 0, s>>>(c64p, c32p, w2re, w2im);
+  P->g64.w2p = c64p;
+  P->g32.w2p = c32p;
   P->g64.X = P->g32.X = P->X;
   P->g64.Y = P->g32.Y = P->Y;
   P->g64.Z = P->g32.Z = P->Z;
   P->g64.N = P->g32.N = N;
+}
+
+extern "C" int fdfd_plan_workspace_bytes(const fdfd_grid_desc* desc, size_t* bytes) {
+  PlanLayout L;
+  TRY(plan_layout(desc, &L));
+  if (!bytes) return set_err(FDFD_ERR_ARG, "bytes is NULL");
+  *bytes = L.total;
+  return 0;
+}
+
+extern "C" int fdfd_plan_create(const fdfd_grid_desc* d, void* ws, size_t ws_bytes, void* stream,
+                                fdfd_plan** out) {
+  PlanLayout L;
+  TRY(plan_layout(d, &L));
+  if (!out) return set_err(FDFD_ERR_ARG, "out is NULL");
+  if (!d->epsilon) return set_err(FDFD_ERR_ARG, "epsilon is NULL");
+  for (int a = 0; a < 3; ++a)
+    if (!d->dxe[a] || !d->dxh[a]) return set_err(FDFD_ERR_ARG, "dxe/dxh[%d] is NULL", a);
+  if (ws_bytes < L.total || (L.total > 0 && !ws))
+    return set_err(FDFD_ERR_WORKSPACE, "plan workspace too small: %zu < %zu", ws_bytes, L.total);
+  if (((uintptr_t)ws & 255) != 0) return set_err(FDFD_ERR_ARG, "plan workspace must be 256-byte aligned");
+  cudaStream_t s = (cudaStream_t)stream;
+  fdfd_plan* P = new fdfd_plan();
+  P->X = d->shape[0];
+  P->Y = d->shape[1];
+  P->Z = d->shape[2];
+  P->N = (long long)P->X * P->Y * P->Z;
+  P->flags = d->flags;
+  P->om_re = d->omega[0];
+  P->om_im = d->omega[1];
+  P->flat = (P->Z == 1);
+  P->has32 = (d->flags & FDFD_GRID_FP32) != 0;
+  P->xc_override[0] = P->xc_override[1] = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&P->nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (P->nsm <= 0) P->nsm = 148;
+  auto cleanup = [&](int rc) {
+    delete P;
+    return rc;
+  };
+  if (cudaStreamCreateWithFlags(&P->cap, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&P->ev[0], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&P->ev[1], cudaEventDisableTiming) != cudaSuccess ||
+      cudaMallocHost((void**)&P->h_poll, 8 * sizeof(int)) != cudaSuccess ||
+      cudaMallocHost((void**)&P->h_state, sizeof(KState)) != cudaSuccess)
+    return cleanup(set_err(FDFD_ERR_CUDA, "plan: stream/event/pinned allocation failed"));
+
+  P->ws = (char*)ws;
+  P->has_mu = d->mu != nullptr;
+  P->has_mask = (d->pec != nullptr) || (d->pmc != nullptr);
+  plan_fill(P, d, L, s);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cleanup(set_err(FDFD_ERR_CUDA, "plan set-up kernels: %s", cudaGetErrorString(e)));
   *out = P;
+  return 0;
+}
+
+extern "C" int fdfd_plan_update(fdfd_plan* P, const fdfd_grid_desc* d, void* stream) {
+  if (!P || !d) return set_err(FDFD_ERR_ARG, "fdfd_plan_update: NULL argument");
+  if (d->shape[0] != P->X || d->shape[1] != P->Y || d->shape[2] != P->Z || d->flags != P->flags ||
+      (d->mu != nullptr) != P->has_mu || ((d->pec != nullptr) || (d->pmc != nullptr)) != P->has_mask)
+    return set_err(FDFD_ERR_ARG, "fdfd_plan_update: shape, flags or optional arrays differ from the plan");
+  if (!d->epsilon) return set_err(FDFD_ERR_ARG, "epsilon is NULL");
+  for (int a = 0; a < 3; ++a)
+    if (!d->dxe[a] || !d->dxh[a]) return set_err(FDFD_ERR_ARG, "dxe/dxh[%d] is NULL", a);
+  PlanLayout L;
+  TRY(plan_layout(d, &L));
+  // captured iteration graphs hold the epsilon pointer: drop them if it moves
+  if (d->epsilon != P->g64.eps) {
+    for (auto& ge : P->graphs) cudaGraphExecDestroy(ge.exec);
+    P->graphs.clear();
+  }
+  plan_fill(P, d, L, (cudaStream_t)stream);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(FDFD_ERR_CUDA, "plan update kernels: %s", cudaGetErrorString(e));
   return 0;
 }
 
@@ -927,7 +976,7 @@ extern "C" int fdfd_eps_gradient(fdfd_plan* P, const void* E, const void* E_adj,
   if (!P || !E || !E_adj || !grad) return set_err(FDFD_ERR_ARG, "fdfd_eps_gradient: NULL argument");
   cudaStream_t s = (cudaStream_t)stream;
   P->launches = 0;
-  OpEpsGrad<double> op{(const cx<double>*)E, (const cx<double>*)E_adj, grad, P->g64.w2, P->g64.mask, P->N};
+  OpEpsGrad<double> op{(const cx<double>*)E, (const cx<double>*)E_adj, grad, P->w2, P->g64.mask, P->N};
   return launch_point<double>(P, P->g64, 0, op, RedBuf{nullptr, nullptr}, s);
 }
 

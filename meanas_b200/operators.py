@@ -108,6 +108,7 @@ class GridOperator:
             self.pec = None if pec is None else as_device(pec, torch.float64, dev, self.n, 'pec')
             self.pmc = None if pmc is None else as_device(pmc, torch.float64, dev, self.n, 'pmc')
             self._keep += dxe + dxh + inv_e + inv_h
+            self._dxe, self._dxh, self._inv_e, self._inv_h = dxe, dxh, inv_e, inv_h
             d = _lib.GridDesc()
             d.shape[:] = self.shape
             d.flags = _lib.GRID_FP32 if fp32 else 0
@@ -131,6 +132,36 @@ class GridOperator:
             self._plan = plan
             self.fp32 = fp32
         self._solve_ws: dict[tuple, torch.Tensor] = {}
+
+    def update(self, omega: complex, dxes, epsilon, mu=None, pec=None, pmc=None) -> None:
+        """Load a new problem of the same shape (and the same optional arrays) into this
+        operator's device buffers and refill the plan in place (``fdfd_plan_update``), so
+        workspaces and captured iteration graphs are reused.  Host inputs are copied on the
+        current stream (asynchronously from pinned tensors)."""
+        if tuple(int(numpy.size(d)) for d in dxes[0]) != self.shape:
+            raise ValueError('update() needs a problem of the same shape')
+        if (mu is None) != (self.mu is None) or (pec is None) != (self.pec is None) or \
+                (pmc is None) != (self.pmc is None):
+            raise ValueError('update() needs the same set of optional arrays (mu, pec, pmc)')
+
+        def put(dst: torch.Tensor, src, dtype, name):
+            if isinstance(src, torch.Tensor):
+                dst.copy_(src.reshape(-1).to(dtype=dtype), non_blocking=src.is_pinned())
+            else:
+                dst.copy_(as_device(src, dtype, self.device, dst.numel(), name))
+        self.omega = complex(omega)
+        with torch.cuda.device(self.device):
+            for a in range(3):
+                put(self._dxe[a], numpy.asarray(dxes[0][a], dtype=complex), torch.complex128, 'dx_e')
+                put(self._dxh[a], numpy.asarray(dxes[1][a], dtype=complex), torch.complex128, 'dx_h')
+                put(self._inv_e[a], 1 / numpy.asarray(dxes[0][a], dtype=complex), torch.complex128, 'dx_e')
+                put(self._inv_h[a], 1 / numpy.asarray(dxes[1][a], dtype=complex), torch.complex128, 'dx_h')
+            put(self.epsilon, epsilon, torch.float64, 'epsilon')
+            for t, src, name in ((self.mu, mu, 'mu'), (self.pec, pec, 'pec'), (self.pmc, pmc, 'pmc')):
+                if t is not None:
+                    put(t, src, torch.float64, name)
+            self._desc.omega[:] = (self.omega.real, self.omega.imag)
+            _lib.check(self.lib.fdfd_plan_update(self.plan, C.byref(self._desc), _stream_handle()))
 
     # ------------------------------------------------------------------ lifetime
     def close(self) -> None:
@@ -222,6 +253,39 @@ class GridOperator:
             ws = torch.empty(int(nbytes.value), dtype=torch.uint8, device=self.device)
             self._solve_ws[key] = ws
         return ws
+
+    def autotune(self, methods=('cocg', 'mixed'), iters: int = 6, candidates=None) -> dict:
+        """Pick the x planes per CTA (the tiling's free parameter: CTA count vs the
+        per-CTA prologue of two extra planes and the tail wave) for each precision by timing
+        ``iters`` iterations of the real solver passes on dense data (a random initial
+        guess), with per-kernel CUDA events.  Returns {precision: (xchunk, us/iteration, all)}."""
+        X = self.shape[0]
+        if candidates is None:
+            candidates = sorted({c for c in (4, 5, 6, 8, 10, 11, 12, 14, 16, 20, 24, 28, 32, 40, 48, 64)
+                                 if c <= max(4, X)} | {min(X, 64)})
+        g = torch.Generator(device=self.device).manual_seed(1)
+        J = torch.zeros(self.n, dtype=torch.complex128, device=self.device)
+        J[self.n // 2] = 1.0
+        guess = torch.randn(self.n, dtype=torch.complex128, device=self.device, generator=g)
+        best = {}
+        for method in methods:
+            prec = 'c64' if method == 'mixed' else 'c128'
+            if method == 'mixed' and not self.fp32:
+                continue
+            kinds = (2, 3) if method == 'mixed' else (0, 1)
+            timing = {}
+            for xc in candidates:
+                self.set_xchunk(prec, xc)
+                kw = dict(method=method, rtol=1e-30, maxiter=iters, criterion='true', profile=True,
+                          max_outer=1)
+                self.solve(J, E_guess=guess, **kw)            # warm-up
+                _, info = self.solve(J, E_guess=guess, **kw)
+                n = max(1, info.kernel_count[kinds[0]])
+                timing[xc] = 1e3 * sum(info.kernel_ms[k] for k in kinds) / n
+            xc = min(timing, key=timing.get)
+            self.set_xchunk(prec, xc)
+            best[prec] = (xc, timing[xc], timing)
+        return best
 
     def release_workspaces(self) -> None:
         self._solve_ws.clear()
