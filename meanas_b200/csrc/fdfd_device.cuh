@@ -57,7 +57,7 @@ template <typename R>
 __device__ __forceinline__ cx<R> czero() { return mkc<R>(R(0), R(0)); }
 
 template <typename R>
-__device__ __forceinline__ cx<R> cld(const cx<R>* p, long long i) { return p[i]; }
+__device__ __forceinline__ cx<R> cld(const cx<R>* p, int i) { return p[i]; }
 
 // Precision conversions.
 __device__ __forceinline__ cx<float> to_c64(cx<double> a) { return mkc<float>((float)a.re, (float)a.im); }
@@ -91,7 +91,7 @@ struct Geo {
   int X, Y, Z;         // cells per axis
   int XC;              // x planes per CTA
   int ntz, nty, nxc;   // CTAs along z tiles, y tiles, x chunks
-  long long N;         // X*Y*Z
+  int N;         // X*Y*Z
   const cx<R>* idxe[3];  // 1/dx_e per axis
   const cx<R>* idxh[3];  // 1/dx_h per axis
   const cx<R>* dxe[3];   // dx_e (for the symmetriser weights p^2)
@@ -215,10 +215,10 @@ __device__ bool grid_reduce(const A (&acc)[NRED], RedBuf rb, double* sh, double*
 //   bool skip() const;             uniform early exit (solver stopped)
 //   void prepare();                read scalars once per thread
 //   const cx<R>* box_src(int b) const;               null = zeros
-//   cx<R> make_u(const cx<R>* v, long long idx, int c) const;   input field from raw values
-//   void stash(const cx<R>* v, long long idx, int c, cx<R>* out) const;  own cell, NS values
-//   void pre(long long cell, Pre& p) const;
-//   void own(long long cell, int i, int j, int k, const cx<R> u[3], const cx<R> y[3],
+//   cx<R> make_u(const cx<R>* v, int idx, int c) const;   input field from raw values
+//   void stash(const cx<R>* v, int idx, int c, cx<R>* out) const;  own cell, NS values
+//   void pre(int cell, Pre& p) const;
+//   void own(int cell, int i, int j, int k, const cx<R> u[3], const cx<R> y[3],
 //            const cx<R> W[3], const cx<R>* st /*[3][NS]*/, const Pre& p, double* acc);
 //   void finish(const double* sums) const;    last CTA, thread 0
 //
@@ -297,8 +297,8 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
   const int j = j0 + ty, k = k0 + tz;
   const bool active = (j < g.Y) && (k < g.Z);
   const int jc = min(j, g.Y - 1), kc = min(k, g.Z - 1);
-  const long long YZ = (long long)g.Y * g.Z;
-  const long long N = g.N;
+  const int YZ = (int)g.Y * g.Z;
+  const int N = g.N;
 
   // slot 0: this thread's own box cell; slot 1: one halo cell (or none)
   const int pos0 = (ty + 1) * BW + tz + KZ;
@@ -360,7 +360,7 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
 
   // issue the asynchronous copies of plane iw's box inputs into Sbox
   auto issue = [&](int iw) {
-    const long long base = (long long)iw * YZ;
+    const int base = (int)iw * YZ;
 #pragma unroll
     for (int bi = 0; bi < NB; ++bi) {
       const cx<R>* src = o.box_src(bi);
@@ -380,19 +380,19 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
   };
   // convert the landed raw inputs of plane iw into U[buf] (and stash own cells)
   auto convert = [&](int buf, int iw, int sb) {  // sb: stash buffer (-1 = none)
-    const long long base = (long long)iw * YZ;
+    const int base = (int)iw * YZ;
 #pragma unroll
     for (int sl = 0; sl < 2; ++sl) {
       const int pos = sl == 0 ? pos0 : pos1;
       if (pos < 0) continue;
-      const long long cell = base + (sl == 0 ? off0 : off1);
+      const int cell = base + (sl == 0 ? off0 : off1);
       const uint8_t m = g.mask ? g.mask[cell] : (uint8_t)0;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         cx<R> v[NB > 0 ? NB : 1];
 #pragma unroll
         for (int bi = 0; bi < NB; ++bi) v[bi] = Sbox[(bi * 3 + c) * BOX + pos];
-        const long long idx = c * N + cell;
+        const int idx = c * N + cell;
         cx<R> u = o.make_u(v, idx, c);
         if (m & (1u << c)) u = czero<R>();
         U[(buf * 3 + c) * BOX + pos] = u;
@@ -407,7 +407,7 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
   };
 
   // H-grid scaling pm * mu^-1 at a cell, per component
-  auto hscale = [&](long long cell, cx<R>& hx, cx<R>& hy, cx<R>& hz) {
+  auto hscale = [&](int cell, cx<R>& hx, cx<R>& hy, cx<R>& hz) {
     if (g.muinv) {
       hx = g.muinv[cell] * hx;
       hy = g.muinv[N + cell] * hy;
@@ -464,7 +464,7 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
   {
     cx<R> hx, hy, hz;
     curl_e(0, 1, ty + 1, tz + KZ, idye, idze, Xt[0], hx, hy, hz);
-    hscale((long long)ip * YZ + (long long)jc * g.Z + kc, hx, hy, hz);
+    hscale((int)ip * YZ + (int)jc * g.Z + kc, hx, hy, hz);
     hy_prev = hy;
     hz_prev = hz;
   }
@@ -472,8 +472,8 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
   for (int i = x0; i < x1; ++i) {
     const int nxt = cur ^ 1;
     const int in1 = (i + 1 == g.X) ? 0 : i + 1;
-    const long long ibase = (long long)i * YZ;
-    const long long cell = ibase + (long long)jc * g.Z + kc;
+    const int ibase = (int)i * YZ;
+    const int cell = ibase + (int)jc * g.Z + kc;
     // own-cell prefetch for this plane's epilogue (latency hidden by the H pass)
     typename Op::Pre pr;
     R e3[3];
@@ -499,7 +499,7 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
     if (row_halo) {  // low y halo row (j0-1)
       cx<R> ax, ay, az;
       curl_e(cur, nxt, 0, tz + KZ, idy_halo, idze, idxe_i, ax, ay, az);
-      hscale(ibase + (long long)jm * g.Z + kh, ax, ay, az);
+      hscale(ibase + (int)jm * g.Z + kh, ax, ay, az);
       Hs[0 * HH * HW + tz + KZ] = ax;
       Hs[1 * HH * HW + tz + KZ] = ay;
       Hs[2 * HH * HW + tz + KZ] = az;
@@ -507,7 +507,7 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
     if (col_halo) {  // low z halo column (k0-1), row j0 + tz
       cx<R> ax, ay, az;
       curl_e(cur, nxt, tz + 1, 0, idy_halo, idze_km, idxe_i, ax, ay, az);
-      hscale(ibase + (long long)jr * g.Z + km, ax, ay, az);
+      hscale(ibase + (int)jr * g.Z + km, ax, ay, az);
       Hs[0 * HH * HW + (tz + 1) * HW] = ax;
       Hs[1 * HH * HW + (tz + 1) * HW] = ay;
       Hs[2 * HH * HW + (tz + 1) * HW] = az;
@@ -564,7 +564,7 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
 
 // ---------------------------------------------------------------- pointwise engine
 // Same CTA geometry without the stencil: own cells of the tile over the x chunk.
-//   void point(long long cell, int i, int j, int k, const cx<R> W[3], double* acc);
+//   void point(int cell, int i, int j, int k, const cx<R> W[3], double* acc);
 template <typename R, int TZ, int TY, class Op>
 __global__ void __launch_bounds__(TZ * TY) k_point(const Geo<R> g, Op op, RedBuf rb) {
   constexpr int NT = TZ * TY;
@@ -580,7 +580,7 @@ __global__ void __launch_bounds__(TZ * TY) k_point(const Geo<R> g, Op op, RedBuf
   const int j = tyb * TY + ty, k = tzb * TZ + tz;
   const int x0 = xcb * g.XC, x1 = min(g.X, x0 + g.XC);
   const bool active = (j < g.Y) && (k < g.Z);
-  const long long YZ = (long long)g.Y * g.Z;
+  const int YZ = (int)g.Y * g.Z;
   WeightYZ<R> wyz;
   if (Op::NEEDS_W) wyz.init(g, min(j, g.Y - 1), min(k, g.Z - 1));
   using A = typename AccT<R>::type;
@@ -593,7 +593,7 @@ __global__ void __launch_bounds__(TZ * TY) k_point(const Geo<R> g, Op op, RedBuf
       cx<R> W[3];
       R aW[3];
       if (Op::NEEDS_W) wyz.at(g.dxe[0][i], g.dxh[0][i], g.adxe[0][i], g.adxh[0][i], W, aW);
-      o.point((long long)i * YZ + (long long)j * g.Z + k, i, j, k, W, aW, acc);
+      o.point((int)i * YZ + (int)j * g.Z + k, i, j, k, W, aW, acc);
     }
   }
   if constexpr (Op::NRED > 0) {

@@ -303,6 +303,10 @@ static int plan_layout(const fdfd_grid_desc* d, PlanLayout* L) {
   for (int a = 0; a < 3; ++a)
     if (d->shape[a] < 1) return set_err(FDFD_ERR_ARG, "shape[%d] = %d must be >= 1", a, d->shape[a]);
   const long long N = (long long)d->shape[0] * d->shape[1] * d->shape[2];
+  // kernels index field elements with 32-bit integers (3N < 2^31: 34 GB per complex128
+  // vector, beyond what a solve's ten vectors can hold on one GPU anyway)
+  if (3 * N > 2147483647LL)
+    return set_err(FDFD_ERR_ARG, "grid of %lld cells is too large: 3*X*Y*Z must be < 2^31", N);
   const long long S = (long long)d->shape[0] + d->shape[1] + d->shape[2];
   const bool f32 = (d->flags & FDFD_GRID_FP32) != 0;
   size_t off = 0;
@@ -700,6 +704,7 @@ struct SolveCtx {
   double tol2;     // on the monitored norm^2
   double bnorm;    // |b|
   int iters, outer, status;
+  int fallbacks;   // mixed -> complex128 COCG switches
 };
 
 static double monitored(const KState& h, int crit) { return crit == 0 ? h.rr : (crit == 1 ? h.rr_pc : h.rr_w2); }
@@ -712,17 +717,18 @@ template <typename RI>
 static int refine_loop(SolveCtx& c, const Geo<RI>& gi, int prec, BsBufs B, double eta, int max_outer, int kind) {
   fdfd_plan* P = c.P;
   cudaStream_t s = c.s;
-  const long long N = P->N;
-  const size_t vb = 3 * N * sizeof(cx<RI>);
+  const int N = (int)P->N;
+  const size_t vb = 3 * (size_t)N * sizeof(cx<RI>);
   const double rscale = c.bnorm > 0 ? 1.0 / c.bnorm : 1.0;
   cx<double>* Ecur = c.x;
   cx<double>* Enext = c.e2;
   cx<RI>* D = (cx<RI>*)B.x;
   bool have_d = false;
-  int local_outer = 0;
+  int local_outer = 0, no_progress = 0;
+  double prev_mon = 0.0;
   for (;;) {
     // the shadow seed is baked into captured graphs, which are keyed by local_outer % 8
-    const unsigned long long seed = 0x5eed5eedULL + 0x9e3779b97f4a7c15ULL * (unsigned long long)(local_outer % 8);
+    const unsigned seed = 0x5eed5eedU + 0x9e3779b9U * (unsigned)(local_outer % 8);
     OpRefine<RI> rf{Ecur, have_d ? D : nullptr, Enext, c.b, (cx<RI>*)B.R0, c.bnorm, rscale, N, seed, c.st};
     TRY(launch_stencil<double>(P, P->g64, 0, rf, c.rb, s));
     std::swap(Ecur, Enext);
@@ -732,7 +738,13 @@ static int refine_loop(SolveCtx& c, const Geo<RI>& gi, int prec, BsBufs B, doubl
     const double mon = monitored(ho, c.crit);
     if (!std::isfinite(mon)) { c.status = ST_NONFINITE; break; }
     if (mon <= c.tol2) { c.status = ST_CONVERGED; break; }
-    if (local_outer >= max_outer || c.iters >= c.o->maxiter) { c.status = ST_MAXITER; break; }
+    if (c.iters >= c.o->maxiter) { c.status = ST_MAXITER; break; }
+    // a refinement step must at least halve the true residual norm^2 ...
+    if (local_outer > 0 && mon > 0.25 * prev_mon) ++no_progress;
+    // ... or the inner precision is not enough for this problem: report it as a
+    // breakdown so the caller can continue in complex128
+    if (no_progress >= 2 || local_outer >= max_outer) { c.status = ST_BREAKDOWN; break; }
+    prev_mon = mon;
     ++local_outer;
     ++c.outer;
     KState hi = make_state(c.o, 0, std::max(1, c.o->maxiter - c.iters), nullptr);
@@ -740,6 +752,8 @@ static int refine_loop(SolveCtx& c, const Geo<RI>& gi, int prec, BsBufs B, doubl
     hi.rr = ho.extra[2];
     hi.bb = ho.extra[2];
     hi.tol2 = eta * eta * ho.extra[2];
+    hi.stall_limit = sizeof(RI) == 4 ? 4000 : 20000;
+    hi.best_rr = ho.extra[2];
     *P->h_state = hi;
     CK(cudaMemcpyAsync(c.st_in, P->h_state, sizeof(KState), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(D, 0, vb, s));
@@ -781,6 +795,101 @@ static int refine_loop(SolveCtx& c, const Geo<RI>& gi, int prec, BsBufs B, doubl
   return 0;
 }
 
+// Complex128 COCG on A0 with the W bilinear form, from the iterate in c.x when
+// `from_x` (else from zero), with random-perturbation restarts after a breakdown and
+// complex128 BiCGSTAB refinement as the last resort.  `gkind` keys its graphs.
+static int cocg_loop(SolveCtx& c, cx<double>* r, cx<double>* q, cx<double>* P0, cx<double>* P1, BsBufs B,
+                     bool from_x, int gkind) {
+  fdfd_plan* P = c.P;
+  const fdfd_solve_opts* o = c.o;
+  cudaStream_t s = c.s;
+  const int N = (int)P->N;
+  const size_t vbytes128 = 3 * (size_t)N * sizeof(double2);
+  const int maxiter = o->maxiter;
+  CK(cudaMemsetAsync(P0, 0, vbytes128, s));
+  {
+    OpCocgInit<double> op{c.b, from_x ? c.x : nullptr, r, N, c.st, 0.0, 0U, nullptr};
+    TRY(launch_stencil<double>(P, P->g64, 0, op, c.rb, s));
+  }
+  KState* st = c.st;
+  RedBuf rb = c.rb;
+  const int chunk = c.chunk;
+  cx<double>* x = c.x;
+  auto enqueue = [&](cudaStream_t ss) -> int {
+    for (int it = 0; it < chunk; ++it) {
+      {
+        ProfScope ps(P, 0, ss);
+        OpCocgA<double> a{r, P0, P1, x, q, N, st};
+        TRY(launch_stencil<double>(P, P->g64, 0, a, rb, ss));
+      }
+      {
+        ProfScope ps(P, 1, ss);
+        OpCocgB<double> bb{r, q, N, st};
+        TRY(launch_point<double>(P, P->g64, 0, bb, rb, ss));
+      }
+    }
+    return 0;
+  };
+  int restarts = 0;
+  for (;;) {
+    CK(cudaMemcpyAsync(P->h_state, st, sizeof(KState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const int left = maxiter - c.iters;
+    if (P->h_state->status == ST_RUNNING && left > 0) {
+      TRY(drive(P, st, chunk, left, s, [&]() -> int {
+        if (o->use_graph && !P->profiling) {
+          P->launches += 2 * chunk;
+          return graph_batch(P, gkind, c.ws, c.x, chunk, s, enqueue);
+        }
+        return enqueue(s);
+      }));
+    }
+    OpCocgFinal<double> fin{P0, P1, x, N, st};
+    TRY(launch_point<double>(P, P->g64, 0, fin, rb, s));
+    CK(cudaMemcpyAsync(P->h_state, st, sizeof(KState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    c.iters += P->h_state->iter;
+    c.status = P->h_state->status;
+    if (c.status == ST_RUNNING) c.status = ST_MAXITER;
+    if (c.status != ST_BREAKDOWN || restarts >= 8 || c.iters >= maxiter) break;
+    // Breakdown: the unconjugated form cancelled (for example a source whose
+    // r^T W r is exactly zero).  Restart COCG from x + s xi, xi a hashed random
+    // vector with |A0 s xi| = 0.1 |r|, which makes the new residual generic.
+    ++restarts;
+    const double rr_before = std::max(P->h_state->rr, 1e-300);
+    const unsigned seed = 0xc0c6U + 0x9e3779b9U * (unsigned)restarts;
+    {
+      OpCocgInit<double> probe{nullptr, nullptr, q, N, st, 1.0, seed, nullptr};
+      TRY(launch_stencil<double>(P, P->g64, 0, probe, rb, s));
+    }
+    CK(cudaMemcpyAsync(P->h_state, st, sizeof(KState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const double axi = std::sqrt(std::max(P->h_state->rr, 1e-300));
+    const double scale = 0.1 * std::sqrt(rr_before) / axi;
+    {
+      OpCocgInit<double> op{c.b, x, r, N, st, scale, seed, c.e2};
+      TRY(launch_stencil<double>(P, P->g64, 0, op, rb, s));
+    }
+    CK(cudaMemcpyAsync(x, c.e2, vbytes128, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemsetAsync(P0, 0, vbytes128, s));
+    // the restarted sequence counts on from c.iters: shift its cap and history
+    KState* hs = P->h_state;
+    CK(cudaMemcpyAsync(hs, st, sizeof(KState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    hs->maxiter = maxiter - c.iters;
+    hs->hist = o->history ? o->history + c.iters : nullptr;
+    CK(cudaMemcpyAsync(st, hs, sizeof(KState), cudaMemcpyHostToDevice, s));
+  }
+  if (c.status == ST_BREAKDOWN || c.status == ST_NONFINITE) {
+    // still stuck: continue from the current iterate with complex128 BiCGSTAB
+    // inside the refinement loop (restarting with fresh shadow vectors).
+    if (c.status == ST_NONFINITE) CK(cudaMemsetAsync(c.x, 0, vbytes128, s));
+    c.status = ST_RUNNING;
+    TRY(refine_loop<double>(c, P->g64, 0, B, 1e-10, 64, 2 + 1000 * c.o->method));
+  }
+  return 0;
+}
+
 // ------------------------------------------------------------------ solve
 extern "C" int fdfd_solve(fdfd_plan* P, const fdfd_solve_opts* o, const void* J, void* E, void* ws,
                           size_t ws_bytes, fdfd_solve_info* info, void* stream) {
@@ -796,8 +905,8 @@ extern "C" int fdfd_solve(fdfd_plan* P, const fdfd_solve_opts* o, const void* J,
   P->ev_marks.clear();
   P->ev_used = 0;
   char* base = (char*)ws;
-  const long long N = P->N;
-  const size_t vbytes128 = 3 * N * sizeof(double2);
+  const int N = (int)P->N;
+  const size_t vbytes128 = 3 * (size_t)N * sizeof(double2);
 
   SolveCtx c;
   c.P = P;
@@ -817,6 +926,7 @@ extern "C" int fdfd_solve(fdfd_plan* P, const fdfd_solve_opts* o, const void* J,
   c.iters = 0;
   c.outer = 0;
   c.status = ST_RUNNING;
+  c.fallbacks = 0;
   const int maxiter = o->maxiter;
   BsBufs B;
   B.R0 = base + L.inner[0];
@@ -853,95 +963,27 @@ extern "C" int fdfd_solve(fdfd_plan* P, const fdfd_solve_opts* o, const void* J,
     cx<double>* q = (cx<double>*)(base + L.cocg[1]);
     cx<double>* P0 = (cx<double>*)(base + L.cocg[2]);
     cx<double>* P1 = (cx<double>*)(base + L.cocg[3]);
-    CK(cudaMemsetAsync(P0, 0, vbytes128, s));
-    {
-      OpCocgInit<double> op{c.b, o->has_guess ? c.x : nullptr, r, N, c.st, 0.0, 0ULL, nullptr};
-      TRY(launch_stencil<double>(P, P->g64, 0, op, c.rb, s));
-    }
-    KState* st = c.st;
-    RedBuf rb = c.rb;
-    const int chunk = c.chunk;
-    cx<double>* x = c.x;
-    auto enqueue = [&](cudaStream_t ss) -> int {
-      for (int it = 0; it < chunk; ++it) {
-        {
-          ProfScope ps(P, 0, ss);
-          OpCocgA<double> a{r, P0, P1, x, q, N, st};
-          TRY(launch_stencil<double>(P, P->g64, 0, a, rb, ss));
-        }
-        {
-          ProfScope ps(P, 1, ss);
-          OpCocgB<double> bb{r, q, N, st};
-          TRY(launch_point<double>(P, P->g64, 0, bb, rb, ss));
-        }
-      }
-      return 0;
-    };
-    int restarts = 0;
-    for (;;) {
-      CK(cudaMemcpyAsync(P->h_state, st, sizeof(KState), cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
-      const int left = maxiter - c.iters;
-      if (P->h_state->status == ST_RUNNING && left > 0) {
-        TRY(drive(P, st, chunk, left, s, [&]() -> int {
-          if (o->use_graph && !P->profiling) {
-            P->launches += 2 * chunk;
-            return graph_batch(P, 0, ws, E, chunk, s, enqueue);
-          }
-          return enqueue(s);
-        }));
-      }
-      OpCocgFinal<double> fin{P0, P1, x, N, st};
-      TRY(launch_point<double>(P, P->g64, 0, fin, rb, s));
-      CK(cudaMemcpyAsync(P->h_state, st, sizeof(KState), cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
-      c.iters += P->h_state->iter;
-      c.status = P->h_state->status;
-      if (c.status == ST_RUNNING) c.status = ST_MAXITER;
-      if (c.status != ST_BREAKDOWN || restarts >= 8 || c.iters >= maxiter) break;
-      // Breakdown: the unconjugated form cancelled (for example a source whose
-      // r^T W r is exactly zero).  Restart COCG from x + s xi, xi a hashed random
-      // vector with |A0 s xi| = 0.1 |r|, which makes the new residual generic.
-      ++restarts;
-      const double rr_before = std::max(P->h_state->rr, 1e-300);
-      const unsigned long long seed = 0xc0c6ULL + 0x9e3779b97f4a7c15ULL * (unsigned long long)restarts;
-      {
-        OpCocgInit<double> probe{nullptr, nullptr, q, N, st, 1.0, seed, nullptr};
-        TRY(launch_stencil<double>(P, P->g64, 0, probe, rb, s));
-      }
-      CK(cudaMemcpyAsync(P->h_state, st, sizeof(KState), cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
-      const double axi = std::sqrt(std::max(P->h_state->rr, 1e-300));
-      const double scale = 0.1 * std::sqrt(rr_before) / axi;
-      {
-        OpCocgInit<double> op{c.b, x, r, N, st, scale, seed, c.e2};
-        TRY(launch_stencil<double>(P, P->g64, 0, op, rb, s));
-      }
-      CK(cudaMemcpyAsync(x, c.e2, vbytes128, cudaMemcpyDeviceToDevice, s));
-      CK(cudaMemsetAsync(P0, 0, vbytes128, s));
-      // the restarted sequence counts on from c.iters: shift its cap and history
-      KState* hs = P->h_state;
-      CK(cudaMemcpyAsync(hs, st, sizeof(KState), cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
-      hs->maxiter = maxiter - c.iters;
-      hs->hist = o->history ? o->history + c.iters : nullptr;
-      CK(cudaMemcpyAsync(st, hs, sizeof(KState), cudaMemcpyHostToDevice, s));
-    }
-    if (c.status == ST_BREAKDOWN || c.status == ST_NONFINITE) {
-      // still stuck: continue from the current iterate with complex128 BiCGSTAB
-      // inside the refinement loop (restarting with fresh shadow vectors).
-      if (c.status == ST_NONFINITE) CK(cudaMemsetAsync(E, 0, vbytes128, s));
-      c.status = ST_RUNNING;
-      TRY(refine_loop<double>(c, P->g64, 0, B, 1e-10, 64, 2));
-    }
+    TRY(cocg_loop(c, r, q, P0, P1, B, o->has_guess != 0, 0));
   } else if (o->method == FDFD_METHOD_MIXED) {
     const double eta = o->inner_rtol > 0 ? o->inner_rtol : 1e-2;
     const int max_outer = o->max_outer > 0 ? o->max_outer : 64;
-    TRY(refine_loop<float>(c, P->g32, 1, B, eta, max_outer, 1));
+    TRY(refine_loop<float>(c, P->g32, 1, B, eta, max_outer, 1 + 1000 * o->method));
+    if (c.status == ST_BREAKDOWN && c.iters < maxiter) {
+      // the complex64 inner solves stopped making progress: finish with complex128
+      // COCG from the current iterate, in the inner solver's memory (eight complex64
+      // vectors hold four complex128 ones)
+      cx<double>* r = (cx<double>*)(base + L.inner[0]);
+      cx<double>* q = (cx<double>*)(base + L.inner[2]);
+      cx<double>* P0 = (cx<double>*)(base + L.inner[4]);
+      cx<double>* P1 = (cx<double>*)(base + L.inner[6]);
+      c.status = ST_RUNNING;
+      ++c.fallbacks;
+      TRY(cocg_loop(c, r, q, P0, P1, B, true, 3 + 1000 * o->method));
+    }
   } else {
     const double eta = o->inner_rtol > 0 ? o->inner_rtol : 1e-10;
     const int max_outer = o->max_outer > 0 ? o->max_outer : 64;
-    TRY(refine_loop<double>(c, P->g64, 0, B, eta, max_outer, 2));
+    TRY(refine_loop<double>(c, P->g64, 0, B, eta, max_outer, 2 + 1000 * o->method));
   }
 
   if (o->adjoint) {
@@ -976,7 +1018,7 @@ extern "C" int fdfd_eps_gradient(fdfd_plan* P, const void* E, const void* E_adj,
   if (!P || !E || !E_adj || !grad) return set_err(FDFD_ERR_ARG, "fdfd_eps_gradient: NULL argument");
   cudaStream_t s = (cudaStream_t)stream;
   P->launches = 0;
-  OpEpsGrad<double> op{(const cx<double>*)E, (const cx<double>*)E_adj, grad, P->w2, P->g64.mask, P->N};
+  OpEpsGrad<double> op{(const cx<double>*)E, (const cx<double>*)E_adj, grad, P->w2, P->g64.mask, (int)P->N};
   return launch_point<double>(P, P->g64, 0, op, RedBuf{nullptr, nullptr}, s);
 }
 

@@ -52,7 +52,11 @@ struct KState {
   int crit;        // 0: monitor rr, 1: monitor rr_pc, 2: monitor rr_w2
   int iter, maxiter, status;
   int pending;     // an x update is still owed (deferred update)
-  int pad;
+  int stall_limit; // BiCGSTAB: stop (ST_BREAKDOWN) after this many iterations without a new
+                   // best residual (0 = never)
+  double best_rr;  // BiCGSTAB: best recurrence residual so far, and its iteration
+  int best_iter;
+  int pad2;
   double* hist;    // relative residual history (length maxiter + 1) or null
 };
 
@@ -100,9 +104,9 @@ __device__ __forceinline__ unsigned hash32(unsigned x) {
 // Element idx of a fixed pseudo-random complex vector (components in [-1/2, 1/2)):
 // BiCGSTAB's shadow vector and the restart perturbation, with no memory traffic.
 template <typename R>
-__device__ __forceinline__ cx<R> shadow(long long idx, unsigned long long seed) {
-  const unsigned a = hash32((unsigned)idx ^ (unsigned)seed);
-  const unsigned b = hash32(a ^ (unsigned)(seed >> 32) ^ 0x9e3779b9U);
+__device__ __forceinline__ cx<R> shadow(int idx, unsigned seed) {
+  const unsigned a = hash32((unsigned)idx ^ seed);
+  const unsigned b = hash32(a ^ ((seed << 16) | (seed >> 16)) ^ 0x9e3779b9U);
   return mkc<R>((R)a * (R)2.3283064365386963e-10 - (R)0.5, (R)b * (R)2.3283064365386963e-10 - (R)0.5);
 }
 // conj(a) * b added to two accumulators of precision A
@@ -140,11 +144,11 @@ struct OpApply {
   __device__ bool skip() const { return false; }
   __device__ void prepare() {}
   __device__ const cx<R>* box_src(int) const { return x; }
-  __device__ void pre(long long, Pre&) const {}
-  __device__ cx<R> pl_at(int c, long long idx) const {
-    const long long N = g.N;
-    const long long cell = idx - c * N;
-    const long long YZ = (long long)g.Y * g.Z;
+  __device__ void pre(int, Pre&) const {}
+  __device__ cx<R> pl_at(int c, int idx) const {
+    const int N = g.N;
+    const int cell = idx - c * N;
+    const int YZ = (int)g.Y * g.Z;
     const int i = (int)(cell / YZ);
     const int j = (int)((cell / g.Z) % g.Y);
     const int k = (int)(cell % g.Z);
@@ -155,7 +159,7 @@ struct OpApply {
     dcx s = csqrt_principal({(double)p2.re, (double)p2.im});
     return mkc<R>((R)s.re, (R)s.im);
   }
-  __device__ cx<R> make_u(const cx<R>* v, long long idx, int c) const {
+  __device__ cx<R> make_u(const cx<R>* v, int idx, int c) const {
     cx<R> u = v[0];
     if (mode == 2) u = cconj(u);
     if (mode >= 1) {
@@ -166,12 +170,12 @@ struct OpApply {
     }
     return u;
   }
-  __device__ void stash(const cx<R>*, long long, int, cx<R>*) const {}
-  __device__ void own(long long cell, int, int, int, const cx<R>*, const cx<R> yv[3], const cx<R>*, const R*,
+  __device__ void stash(const cx<R>*, int, int, cx<R>*) const {}
+  __device__ void own(int cell, int, int, int, const cx<R>*, const cx<R> yv[3], const cx<R>*, const R*,
                       const cx<R>*, const Pre&, acc_t<R>*) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const long long idx = c * g.N + cell;
+      const int idx = c * g.N + cell;
       cx<R> v = yv[c];
       if (mode >= 1) v = pl_at(c, idx) * v;
       if (mode == 2) v = cconj(v);
@@ -198,15 +202,15 @@ struct OpRhs {
   double om_re, om_im;
   int adjoint;
   const uint8_t* mask;
-  long long N;
+  int N;
   KState* st;
   __device__ bool skip() const { return false; }
   __device__ void prepare() {}
-  __device__ void point(long long cell, int, int, int, const cx<R> W[3], const R aW[3], acc_t<R>* acc) const {
+  __device__ void point(int cell, int, int, int, const cx<R> W[3], const R aW[3], acc_t<R>* acc) const {
     const uint8_t m = mask ? mask[cell] : (uint8_t)0;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const long long idx = c * N + cell;
+      const int idx = c * N + cell;
       const cx<R> j = J[idx];
       // -i * omega * J
       const cx<R> b0 = mkc<R>((R)(om_im * j.re + om_re * j.im), (R)(om_im * j.im - om_re * j.re));
@@ -246,13 +250,13 @@ struct OpAdjPost {
   static constexpr int NRED = 0;
   static constexpr bool NEEDS_W = true;
   cx<R>* x;
-  long long N;
+  int N;
   __device__ bool skip() const { return false; }
   __device__ void prepare() {}
-  __device__ void point(long long cell, int, int, int, const cx<R> W[3], const R*, acc_t<R>*) const {
+  __device__ void point(int cell, int, int, int, const cx<R> W[3], const R*, acc_t<R>*) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const long long idx = c * N + cell;
+      const int idx = c * N + cell;
       x[idx] = cconj(W[c] * x[idx]);
     }
   }
@@ -270,10 +274,10 @@ struct OpCocgInit {
   const cx<R>* b;   // may be null (zero)
   const cx<R>* x;   // may be null (zero guess)
   cx<R>* r;
-  long long N;
+  int N;
   KState* st;
   double pert;
-  unsigned long long seed;
+  unsigned seed;
   cx<R>* xnew;      // may be null
   struct Pre {
     cx<R> b[3];
@@ -281,21 +285,21 @@ struct OpCocgInit {
   __device__ bool skip() const { return false; }
   __device__ void prepare() {}
   __device__ const cx<R>* box_src(int) const { return x; }
-  __device__ void pre(long long cell, Pre& p) const {
+  __device__ void pre(int cell, Pre& p) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) p.b[c] = b ? b[c * N + cell] : czero<R>();
   }
-  __device__ cx<R> make_u(const cx<R>* v, long long idx, int) const {
+  __device__ cx<R> make_u(const cx<R>* v, int idx, int) const {
     cx<R> u = v[0];
     if (pert != 0.0) u = caxpy(mkc<R>((R)pert, R(0)), shadow<R>(idx, seed), u);
     return u;
   }
-  __device__ void stash(const cx<R>*, long long, int, cx<R>*) const {}
-  __device__ void own(long long cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R> W[3],
+  __device__ void stash(const cx<R>*, int, int, cx<R>*) const {}
+  __device__ void own(int cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R> W[3],
                       const R aW[3], const cx<R>*, const Pre& pr, acc_t<R>* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const long long idx = c * N + cell;
+      const int idx = c * N + cell;
       const cx<R> rv = pr.b[c] - y[c];
       r[idx] = rv;
       if (xnew) xnew[idx] = u[c];
@@ -334,7 +338,7 @@ struct OpCocgA {
   cx<R>* P1;
   cx<R>* x;
   cx<R>* q;
-  long long N;
+  int N;
   KState* st;
   // per-thread
   const cx<R>* p_old;
@@ -354,18 +358,18 @@ struct OpCocgA {
     upd = __ldcg(&st->pending) != 0;
   }
   __device__ const cx<R>* box_src(int bi) const { return bi == 0 ? r : p_old; }
-  __device__ void pre(long long cell, Pre& p) const {
+  __device__ void pre(int cell, Pre& p) const {
     if (!upd) return;
 #pragma unroll
     for (int c = 0; c < 3; ++c) p.x[c] = x[c * N + cell];
   }
-  __device__ cx<R> make_u(const cx<R>* v, long long, int) const { return caxpy(beta, v[1], v[0]); }
-  __device__ void stash(const cx<R>* v, long long, int, cx<R>* out) const { out[0] = v[1]; }
-  __device__ void own(long long cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R> W[3],
+  __device__ cx<R> make_u(const cx<R>* v, int, int) const { return caxpy(beta, v[1], v[0]); }
+  __device__ void stash(const cx<R>* v, int, int, cx<R>* out) const { out[0] = v[1]; }
+  __device__ void own(int cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R> W[3],
                       const R*, const cx<R>* sv, const Pre& pr, acc_t<R>* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const long long idx = c * N + cell;
+      const int idx = c * N + cell;
       if (upd) x[idx] = caxpy(alpha, sv[c], pr.x[c]);
       p_new[idx] = u[c];
       q[idx] = y[c];
@@ -399,7 +403,7 @@ struct OpCocgB {
   static constexpr bool NEEDS_W = true;
   cx<R>* r;
   const cx<R>* q;
-  long long N;
+  int N;
   KState* st;
   cx<R> malpha;
   __device__ bool skip() const { return ld_status(st) != ST_RUNNING; }
@@ -407,10 +411,10 @@ struct OpCocgB {
     const dcx a = ld_dcx(&st->alpha);
     malpha = mkc<R>((R)(-a.re), (R)(-a.im));
   }
-  __device__ void point(long long cell, int, int, int, const cx<R> W[3], const R aW[3], acc_t<R>* acc) const {
+  __device__ void point(int cell, int, int, int, const cx<R> W[3], const R aW[3], acc_t<R>* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const long long idx = c * N + cell;
+      const int idx = c * N + cell;
       const cx<R> rv = caxpy(malpha, q[idx], r[idx]);
       r[idx] = rv;
       const cx<R> wr = W[c] * rv;
@@ -460,7 +464,7 @@ struct OpCocgFinal {
   cx<R>* P0;
   cx<R>* P1;
   cx<R>* x;
-  long long N;
+  int N;
   KState* st;
   const cx<R>* p;
   cx<R> alpha;
@@ -472,11 +476,11 @@ struct OpCocgFinal {
     alpha = from_d<R>(ld_dcx(&st->alpha));
     upd = __ldcg(&st->pending) != 0;
   }
-  __device__ void point(long long cell, int, int, int, const cx<R>*, const R*, acc_t<R>*) const {
+  __device__ void point(int cell, int, int, int, const cx<R>*, const R*, acc_t<R>*) const {
     if (!upd) return;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const long long idx = c * N + cell;
+      const int idx = c * N + cell;
       x[idx] = caxpy(alpha, p[idx], x[idx]);
     }
   }
@@ -505,8 +509,8 @@ struct OpBsP {
   static constexpr int NB = 4, NS = 2, NRED = 3;
   static constexpr bool NEEDS_W = false;
   BsBufs B;
-  long long N;
-  unsigned long long seed;
+  int N;
+  unsigned seed;
   KState* st;
   const cx<R>* ro;
   const cx<R>* vo;
@@ -550,20 +554,20 @@ struct OpBsP {
     if (!upd && bi > 0) return nullptr;
     return bi == 0 ? ro : (bi == 1 ? vo : (bi == 2 ? t : po));
   }
-  __device__ void pre(long long cell, Pre& p) const {
+  __device__ void pre(int cell, Pre& p) const {
     if (!upd) return;
 #pragma unroll
     for (int c = 0; c < 3; ++c) p.x[c] = x[c * N + cell];
   }
   // v = [r_old, v_old, t, p_old]
-  __device__ cx<R> make_u(const cx<R>* v, long long, int) const {
+  __device__ cx<R> make_u(const cx<R>* v, int, int) const {
     if (!upd) return v[0];
     const cx<R> s = caxpy(malpha, v[1], v[0]);
     const cx<R> r = caxpy(momega, v[2], s);
     return caxpy(beta, caxpy(momega, v[1], v[3]), r);
   }
   // stash: r_new and the owed x update alpha p_old + omega s
-  __device__ void stash(const cx<R>* v, long long, int, cx<R>* out) const {
+  __device__ void stash(const cx<R>* v, int, int, cx<R>* out) const {
     if (!upd) {
       out[0] = v[0];
       out[1] = czero<R>();
@@ -573,11 +577,11 @@ struct OpBsP {
     out[0] = caxpy(momega, v[2], s);
     out[1] = caxpy(omega, s, alpha * v[3]);
   }
-  __device__ void own(long long cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R>*, const R*,
+  __device__ void own(int cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R>*, const R*,
                       const cx<R>* sv, const Pre& pr, acc_t<R>* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const long long idx = c * N + cell;
+      const int idx = c * N + cell;
       const cx<R> r = sv[c * 2 + 0];
       if (upd) x[idx] = pr.x[c] + sv[c * 2 + 1];
       rn[idx] = r;
@@ -610,8 +614,8 @@ struct OpBsS {
   static constexpr int NB = 2, NS = 0, NRED = 6;
   static constexpr bool NEEDS_W = false;
   BsBufs B;
-  long long N;
-  unsigned long long seed;
+  int N;
+  unsigned seed;
   KState* st;
   const cx<R>* r;
   const cx<R>* v;
@@ -628,14 +632,14 @@ struct OpBsS {
     malpha = mkc<R>((R)(-a.re), (R)(-a.im));
   }
   __device__ const cx<R>* box_src(int bi) const { return bi == 0 ? r : v; }
-  __device__ void pre(long long, Pre&) const {}
-  __device__ cx<R> make_u(const cx<R>* vv, long long, int) const { return caxpy(malpha, vv[1], vv[0]); }
-  __device__ void stash(const cx<R>*, long long, int, cx<R>*) const {}
-  __device__ void own(long long cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R>*, const R*,
+  __device__ void pre(int, Pre&) const {}
+  __device__ cx<R> make_u(const cx<R>* vv, int, int) const { return caxpy(malpha, vv[1], vv[0]); }
+  __device__ void stash(const cx<R>*, int, int, cx<R>*) const {}
+  __device__ void own(int cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R>*, const R*,
                       const cx<R>*, const Pre&, acc_t<R>* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const long long idx = c * N + cell;
+      const int idx = c * N + cell;
       t[idx] = y[c];
       acc_cdot<R>(acc, y[c], u[c]);                       // (t, s)
       acc[2] += cabs2(y[c]);                              // |t|^2
@@ -670,6 +674,14 @@ struct OpBsS {
     st->rr = rr;
     check_progress(st, rr, true);
     if (st->status != ST_RUNNING) return;
+    // stagnation: no 1 % improvement on the best residual for stall_limit iterations
+    if (rr < 0.98 * st->best_rr || st->iter == 1) {
+      st->best_rr = rr;
+      st->best_iter = st->iter;
+    } else if (st->stall_limit > 0 && st->iter - st->best_iter >= st->stall_limit) {
+      st->status = ST_BREAKDOWN;
+      return;
+    }
     const dcx rho_new = {-(om.re * rht.re - om.im * rht.im), -(om.re * rht.im + om.im * rht.re)};
     if (dabs(om) <= 1e-300 || dabs(rho_new) <= 1e-300) {
       st->status = ST_BREAKDOWN;
@@ -689,8 +701,8 @@ struct OpBsInit {
   const cx<R>* b;
   const cx<R>* x;
   cx<R>* r;
-  long long N;
-  unsigned long long seed;
+  int N;
+  unsigned seed;
   KState* st;
   struct Pre {
     cx<R> b[3];
@@ -698,17 +710,17 @@ struct OpBsInit {
   __device__ bool skip() const { return false; }
   __device__ void prepare() {}
   __device__ const cx<R>* box_src(int) const { return x; }
-  __device__ void pre(long long cell, Pre& p) const {
+  __device__ void pre(int cell, Pre& p) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) p.b[c] = b[c * N + cell];
   }
-  __device__ cx<R> make_u(const cx<R>* v, long long, int) const { return v[0]; }
-  __device__ void stash(const cx<R>*, long long, int, cx<R>*) const {}
-  __device__ void own(long long cell, int, int, int, const cx<R>*, const cx<R> y[3], const cx<R>*, const R*,
+  __device__ cx<R> make_u(const cx<R>* v, int, int) const { return v[0]; }
+  __device__ void stash(const cx<R>*, int, int, cx<R>*) const {}
+  __device__ void own(int cell, int, int, int, const cx<R>*, const cx<R> y[3], const cx<R>*, const R*,
                       const cx<R>*, const Pre& pr, acc_t<R>* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const long long idx = c * N + cell;
+      const int idx = c * N + cell;
       const cx<R> rv = pr.b[c] - y[c];
       r[idx] = rv;
       acc_cdot<R>(acc, shadow<R>(idx, seed), rv);
@@ -733,7 +745,7 @@ struct OpBsFinal {
   static constexpr int NRED = 0;
   static constexpr bool NEEDS_W = false;
   BsBufs B;
-  long long N;
+  int N;
   KState* st;
   const cx<R>* r;
   const cx<R>* v;
@@ -753,11 +765,11 @@ struct OpBsFinal {
     omega = from_d<R>(ld_dcx(&st->omega));
     malpha = mkc<R>(-alpha.re, -alpha.im);
   }
-  __device__ void point(long long cell, int, int, int, const cx<R>*, const R*, acc_t<R>*) const {
+  __device__ void point(int cell, int, int, int, const cx<R>*, const R*, acc_t<R>*) const {
     if (!upd) return;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const long long idx = c * N + cell;
+      const int idx = c * N + cell;
       const cx<R> s = caxpy(malpha, v[idx], r[idx]);
       x[idx] = caxpy(omega, s, caxpy(alpha, p[idx], x[idx]));
     }
@@ -779,8 +791,8 @@ struct OpRefine {
   const cx<double>* b;
   cx<RI>* rin;
   double scale, rscale;
-  long long N;
-  unsigned long long seed;
+  int N;
+  unsigned seed;
   KState* st;
   struct Pre {
     cx<double> b[3];
@@ -788,11 +800,11 @@ struct OpRefine {
   __device__ bool skip() const { return false; }
   __device__ void prepare() {}
   __device__ const cx<double>* box_src(int) const { return E_old; }
-  __device__ void pre(long long cell, Pre& p) const {
+  __device__ void pre(int cell, Pre& p) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) p.b[c] = b[c * N + cell];
   }
-  __device__ cx<double> make_u(const cx<double>* v, long long idx, int) const {
+  __device__ cx<double> make_u(const cx<double>* v, int idx, int) const {
     cx<double> e = v[0];
     if (d) {
       const cx<RI> dv = d[idx];
@@ -800,12 +812,12 @@ struct OpRefine {
     }
     return e;
   }
-  __device__ void stash(const cx<double>*, long long, int, cx<double>*) const {}
-  __device__ void own(long long cell, int, int, int, const cx<double> u[3], const cx<double> y[3],
+  __device__ void stash(const cx<double>*, int, int, cx<double>*) const {}
+  __device__ void own(int cell, int, int, int, const cx<double> u[3], const cx<double> y[3],
                       const cx<double>*, const double aW[3], const cx<double>*, const Pre& pr, double* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const long long idx = c * N + cell;
+      const int idx = c * N + cell;
       E_new[idx] = u[c];
       const cx<double> rv = pr.b[c] - y[c];
       const cx<RI> r1 = mkc<RI>((RI)(rscale * rv.re), (RI)(rscale * rv.im));
@@ -848,13 +860,13 @@ struct OpResidual {
   __device__ bool skip() const { return false; }
   __device__ void prepare() {}
   __device__ const cx<R>* box_src(int) const { return E; }
-  __device__ void pre(long long cell, Pre& p) const {
+  __device__ void pre(int cell, Pre& p) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) p.j[c] = J[c * g.N + cell];
   }
-  __device__ cx<R> w_at(int c, long long idx) const {
-    const long long cell = idx - c * g.N;
-    const long long YZ = (long long)g.Y * g.Z;
+  __device__ cx<R> w_at(int c, int idx) const {
+    const int cell = idx - c * g.N;
+    const int YZ = (int)g.Y * g.Z;
     const int i = (int)(cell / YZ);
     const int j = (int)((cell / g.Z) % g.Y);
     const int k = (int)(cell % g.Z);
@@ -862,7 +874,7 @@ struct OpResidual {
     if (c == 1) return g.dxh[0][i] * g.dxe[1][j] * g.dxh[2][k];
     return g.dxh[0][i] * g.dxh[1][j] * g.dxe[2][k];
   }
-  __device__ cx<R> make_u(const cx<R>* v, long long idx, int c) const {
+  __device__ cx<R> make_u(const cx<R>* v, int idx, int c) const {
     cx<R> e = v[0];
     if (adjoint) {
       const cx<R> w = w_at(c, idx);
@@ -871,8 +883,8 @@ struct OpResidual {
     }
     return e;
   }
-  __device__ void stash(const cx<R>*, long long, int, cx<R>*) const {}
-  __device__ void own(long long, int, int, int, const cx<R>*, const cx<R> y[3], const cx<R> W[3],
+  __device__ void stash(const cx<R>*, int, int, cx<R>*) const {}
+  __device__ void own(int, int, int, int, const cx<R>*, const cx<R> y[3], const cx<R> W[3],
                       const R aW[3], const cx<R>*, const Pre& pr, acc_t<R>* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -908,14 +920,14 @@ struct OpEpsGrad {
   R* grad;
   cx<R> w2;
   const uint8_t* mask;
-  long long N;
+  int N;
   __device__ bool skip() const { return false; }
   __device__ void prepare() {}
-  __device__ void point(long long cell, int, int, int, const cx<R>*, const R*, acc_t<R>*) const {
+  __device__ void point(int cell, int, int, int, const cx<R>*, const R*, acc_t<R>*) const {
     const uint8_t m = mask ? mask[cell] : (uint8_t)0;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const long long idx = c * N + cell;
+      const int idx = c * N + cell;
       const cx<R> v = w2 * (cconj(Ea[idx]) * E[idx]);
       grad[idx] = (m & (1u << c)) ? R(0) : v.re;
     }
@@ -930,13 +942,13 @@ struct OpCopy {
   static constexpr bool NEEDS_W = false;
   const cx<RS>* src;  // null = zero fill
   cx<RD>* dst;
-  long long N;
+  int N;
   __device__ bool skip() const { return false; }
   __device__ void prepare() {}
-  __device__ void point(long long cell, int, int, int, const void*, const void*, acc_t<RD>*) const {
+  __device__ void point(int cell, int, int, int, const void*, const void*, acc_t<RD>*) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const long long idx = c * N + cell;
+      const int idx = c * N + cell;
       if (src) {
         const cx<RS> v = src[idx];
         dst[idx] = mkc<RD>((RD)v.re, (RD)v.im);

@@ -100,7 +100,7 @@ class FDFDServer:
     """
 
     def __init__(self, device: Any | None = None, *, max_active: int = 8, hbm_budget: int | None = None,
-                 precision: str = 'mixed', rtol: float = 1e-8, maxiter: int | None = None,
+                 precision: str = 'mixed', rtol: float = 1e-8, maxiter: int | None = 200000,
                  xchunk: int | None = None):
         self.device = torch.device(device) if device is not None else torch.device('cuda', 0)
         self._slot_factory = _Slot
