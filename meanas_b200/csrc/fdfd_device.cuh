@@ -208,23 +208,26 @@ __device__ bool grid_reduce(const A (&acc)[NRED], RedBuf rb, double* sh, double*
 // ---------------------------------------------------------------- stencil engine
 // Op interface:
 //   static constexpr int NB;       box inputs: complex 3N vectors read on the tile + halo
-//   static constexpr int NS;       complex values per component stashed for own cells
+//   static constexpr int NO;       own inputs: complex 3N vectors read on own cells only
 //   static constexpr int NRED;     number of FP64 accumulators (0 = none)
 //   static constexpr bool NEEDS_W; pass symmetriser weights to own()
 //   struct Pre;                    own-cell values prefetched at the start of a plane step
 //   bool skip() const;             uniform early exit (solver stopped)
 //   void prepare();                read scalars once per thread
 //   const cx<R>* box_src(int b) const;               null = zeros
+//   const cx<R>* own_src(int o) const;               null = zeros
 //   cx<R> make_u(const cx<R>* v, int idx, int c) const;   input field from raw values
-//   void stash(const cx<R>* v, int idx, int c, cx<R>* out) const;  own cell, NS values
+//   void convert_own(const cx<R>* v, const cx<R>* ov, int idx, int c, cx<R> u, A* acc) const;
+//        own cells of the CTA's planes, when their inputs land: outputs that do not need
+//        the operator (p = r + beta p_old, x updates, r updates) are written here
 //   void pre(int cell, Pre& p) const;
 //   void own(int cell, int i, int j, int k, const cx<R> u[3], const cx<R> y[3],
-//            const cx<R> W[3], const cx<R>* st /*[3][NS]*/, const Pre& p, double* acc);
+//            const cx<R> W[3], const R aW[3], const Pre& p, A* acc);   y = A0 u
 //   void finish(const double* sums) const;    last CTA, thread 0
 //
-// Pipeline per x plane i (U holds u on planes i and i+1, Sbox the raw inputs of plane
-// i+2 in flight):  wait for plane i+1's copies -> convert them into U (u = make_u,
-// PEC mask; own cells also stash) -> issue cp.async for plane i+2 -> H = ce(u) on the
+// Pipeline per x plane i (U holds u on planes i and i+1, Sbox/Sown the raw inputs of
+// plane i+2 in flight):  wait for plane i+1's copies -> convert them into U (u = make_u,
+// PEC mask; own cells: convert_own) -> issue cp.async for plane i+2 -> H = ce(u) on the
 // tile + low halo -> curl of H, epilogue.  Global loads of the box are asynchronous
 // copies, so they overlap the arithmetic of the previous plane.
 __device__ __forceinline__ void cp_async16(void* s, const void* g) {
@@ -247,7 +250,7 @@ __device__ __forceinline__ void cp_async_cx(cx<R>* s, const cx<R>* g) {
 // Upper bound on x planes per CTA (per-CTA plane tables live in shared memory).
 constexpr int XC_MAX = 64;
 
-template <typename R, int TZ, int TY, bool FLAT, int NB, int NS>
+template <typename R, int TZ, int TY, bool FLAT, int NB, int NO>
 struct StencilShape {
   static constexpr int NT = TZ * TY;
   static constexpr int KZ = FLAT ? 0 : 1;      // z offset of own cells inside the box
@@ -257,9 +260,9 @@ struct StencilShape {
   static constexpr int NHALO = BOX - NT;       // halo cells (<= NT)
   static constexpr int HW = TZ + KZ;           // H plane width (own + low z halo)
   static constexpr int HH = TY + 1;
-  // shared memory: Sbox[NB][3][BOX] | Sraw[2][NS][3][NT] | U[2][3][BOX] | Hs[3][HH*HW] | red[64]
-  static constexpr size_t off_raw = sizeof(cx<R>) * (size_t)NB * 3 * BOX;
-  static constexpr size_t off_u = off_raw + sizeof(cx<R>) * (size_t)2 * NS * 3 * NT;  // NS may be 0
+  // shared memory: Sbox[NB][3][BOX] | Sown[NO][3][NT] | U[2][3][BOX] | Hs[3][HH*HW] | Xt | red[64]
+  static constexpr size_t off_own = sizeof(cx<R>) * (size_t)NB * 3 * BOX;
+  static constexpr size_t off_u = off_own + sizeof(cx<R>) * (size_t)NO * 3 * NT;
   static constexpr size_t off_h = off_u + sizeof(cx<R>) * (size_t)2 * 3 * BOX;
   static constexpr size_t off_xt = off_h + sizeof(cx<R>) * (size_t)3 * HH * HW;
   static constexpr int XT_STRIDE = 6;  // per plane: idxe, idxh, dxe, dxh, (|dxe|, |dxh|)
@@ -270,12 +273,12 @@ struct StencilShape {
 
 template <typename R, int TZ, int TY, bool FLAT, int MINB, class Op>
 __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op, RedBuf rb) {
-  using S = StencilShape<R, TZ, TY, FLAT, Op::NB, Op::NS>;
+  using S = StencilShape<R, TZ, TY, FLAT, Op::NB, Op::NO>;
   constexpr int NT = S::NT, BW = S::BW, BOX = S::BOX, KZ = S::KZ, HW = S::HW, HH = S::HH;
-  constexpr int NB = Op::NB, NS = Op::NS > 0 ? Op::NS : 1;
+  constexpr int NB = Op::NB, NO = Op::NO;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* Sbox = reinterpret_cast<cx<R>*>(smem_raw);                 // [NB][3][BOX]
-  cx<R>* Sraw = reinterpret_cast<cx<R>*>(smem_raw + S::off_raw);    // [2][NS][3][NT]
+  cx<R>* Sown = reinterpret_cast<cx<R>*>(smem_raw + S::off_own);    // [NO][3][NT]
   cx<R>* U = reinterpret_cast<cx<R>*>(smem_raw + S::off_u);         // [2][3][BOX]
   cx<R>* Hs = reinterpret_cast<cx<R>*>(smem_raw + S::off_h);        // [3][HH*HW]
   cx<R>* Xt = reinterpret_cast<cx<R>*>(smem_raw + S::off_xt);       // [XC+1][6]
@@ -376,10 +379,21 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
         }
       }
     }
+#pragma unroll
+    for (int oi = 0; oi < NO; ++oi) {
+      const cx<R>* src = o.own_src(oi);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        cx<R>* dst = Sown + (oi * 3 + c) * NT + tid;
+        if (src) cp_async_cx<R>(dst, src + c * N + base + off0);
+        else *dst = czero<R>();
+      }
+    }
     cp_async_commit();
   };
-  // convert the landed raw inputs of plane iw into U[buf] (and stash own cells)
-  auto convert = [&](int buf, int iw, int sb) {  // sb: stash buffer (-1 = none)
+  // convert the landed raw inputs of plane iw into U[buf]; own cells of the CTA's own
+  // planes (own_plane) also run the op's convert_own
+  auto convert = [&](int buf, int iw, bool own_plane) {
     const int base = (int)iw * YZ;
 #pragma unroll
     for (int sl = 0; sl < 2; ++sl) {
@@ -396,11 +410,11 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
         cx<R> u = o.make_u(v, idx, c);
         if (m & (1u << c)) u = czero<R>();
         U[(buf * 3 + c) * BOX + pos] = u;
-        if (Op::NS > 0 && sl == 0 && sb >= 0) {
-          cx<R> st[NS];
-          o.stash(v, idx, c, st);
+        if (sl == 0 && own_plane && active) {
+          cx<R> ov[NO > 0 ? NO : 1];
 #pragma unroll
-          for (int q = 0; q < Op::NS; ++q) Sraw[((sb * NS + q) * 3 + c) * NT + tid] = st[q];
+          for (int oi = 0; oi < NO; ++oi) ov[oi] = Sown[(oi * 3 + c) * NT + tid];
+          o.convert_own(v, ov, idx, c, u, acc);
         }
       }
     }
@@ -451,12 +465,12 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
   issue(ip);
   cp_async_wait_all();
   __syncthreads();
-  convert(0, ip, -1);
+  convert(0, ip, false);
   __syncthreads();
   issue(x0);
   cp_async_wait_all();
   __syncthreads();
-  convert(1, x0, 0);
+  convert(1, x0, true);
   __syncthreads();
   // plane x0+1 starts landing while the prologue H is computed
   issue(x0 + 1 == g.X ? 0 : x0 + 1);
@@ -484,7 +498,7 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
     }
     cp_async_wait_all();   // plane i+1 landed
     __syncthreads();       // ... for everyone; U[nxt] (plane i-1) and Hs no longer read
-    convert(nxt, in1, (i + 1 - x0) & 1);
+    convert(nxt, in1, i + 1 < x1);
     __syncthreads();       // U[nxt] = u(i+1) ready; Sbox free
     if (i + 1 < x1) issue(in1 + 1 == g.X ? 0 : in1 + 1);
     const cx<R>* xe = Xt + (i - x0 + 1) * S::XT_STRIDE;
@@ -543,14 +557,7 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
       cx<R> W[3];
       R aW[3];
       if (Op::NEEDS_W) wyz.at(xe[2], xe[3], xe[4].re, xe[4].im, W, aW);
-      cx<R> st[3 * NS];
-      if (Op::NS > 0) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-#pragma unroll
-          for (int q = 0; q < Op::NS; ++q) st[c * NS + q] = Sraw[((((i - x0) & 1) * NS + q) * 3 + c) * NT + tid];
-      }
-      o.own(cell, i, j, k, u, y, W, aW, st, pr, acc);
+      o.own(cell, i, j, k, u, y, W, aW, pr, acc);
     }
     cur = nxt;
   }

@@ -253,12 +253,12 @@ static int launch_stencil(fdfd_plan* P, const Geo<R>& g0, int precision, const O
   const Tiling t = make_tiling(P, precision);
   const Geo<R> g = geo_with(g0, t);
   if (P->flat) {
-    using Sh = StencilShape<R, 1, FLAT_TY, true, Op::NB, Op::NS>;
+    using Sh = StencilShape<R, 1, FLAT_TY, true, Op::NB, Op::NO>;
     auto kern = k_stencil<R, 1, FLAT_TY, true, MinBlocks<R>::value, Op>;
     ensure_smem(kern, Sh::smem_bytes());
     kern<<<(unsigned)t.nblocks, dim3(1, FLAT_TY), Sh::smem_bytes(), s>>>(g, op, rb);
   } else {
-    using Sh = StencilShape<R, TZ3, TY3, false, Op::NB, Op::NS>;
+    using Sh = StencilShape<R, TZ3, TY3, false, Op::NB, Op::NO>;
     auto kern = k_stencil<R, TZ3, TY3, false, MinBlocks<R>::value, Op>;
     ensure_smem(kern, Sh::smem_bytes());
     kern<<<(unsigned)t.nblocks, dim3(TZ3, TY3), Sh::smem_bytes(), s>>>(g, op, rb);

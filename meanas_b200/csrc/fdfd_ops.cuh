@@ -134,7 +134,7 @@ __device__ __forceinline__ dcx csqrt_principal(dcx z) {
 
 template <typename R>
 struct OpApply {
-  static constexpr int NB = 1, NS = 0, NRED = 0;
+  static constexpr int NB = 1, NO = 0, NRED = 0;
   static constexpr bool NEEDS_W = false;
   const cx<R>* x;
   cx<R>* y;
@@ -170,9 +170,10 @@ struct OpApply {
     }
     return u;
   }
-  __device__ void stash(const cx<R>*, int, int, cx<R>*) const {}
+  __device__ const cx<R>* own_src(int) const { return nullptr; }
+  __device__ void convert_own(const cx<R>*, const cx<R>*, int, int, cx<R>, acc_t<R>*) const {}
   __device__ void own(int cell, int, int, int, const cx<R>*, const cx<R> yv[3], const cx<R>*, const R*,
-                      const cx<R>*, const Pre&, acc_t<R>*) const {
+                      const Pre&, acc_t<R>*) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int idx = c * g.N + cell;
@@ -269,7 +270,7 @@ struct OpAdjPost {
 // reduces r^T W r, |r|^2, sum|W||r|^2, sum|W|^2|r|^2.
 template <typename R>
 struct OpCocgInit {
-  static constexpr int NB = 1, NS = 0, NRED = 5;
+  static constexpr int NB = 1, NO = 0, NRED = 5;
   static constexpr bool NEEDS_W = true;
   const cx<R>* b;   // may be null (zero)
   const cx<R>* x;   // may be null (zero guess)
@@ -294,15 +295,15 @@ struct OpCocgInit {
     if (pert != 0.0) u = caxpy(mkc<R>((R)pert, R(0)), shadow<R>(idx, seed), u);
     return u;
   }
-  __device__ void stash(const cx<R>*, int, int, cx<R>*) const {}
+  __device__ const cx<R>* own_src(int) const { return nullptr; }
+  __device__ void convert_own(const cx<R>*, const cx<R>*, int, int, cx<R>, acc_t<R>*) const {}
   __device__ void own(int cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R> W[3],
-                      const R aW[3], const cx<R>*, const Pre& pr, acc_t<R>* acc) const {
+                      const R aW[3], const Pre& pr, acc_t<R>* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int idx = c * N + cell;
       const cx<R> rv = pr.b[c] - y[c];
       r[idx] = rv;
-      if (xnew) xnew[idx] = u[c];
       const cx<R> wr = W[c] * rv;
       acc[0] += (double)wr.re * (double)rv.re - (double)wr.im * (double)rv.im;
       acc[1] += (double)wr.re * (double)rv.im + (double)wr.im * (double)rv.re;
@@ -331,7 +332,7 @@ struct OpCocgInit {
 // p = r + beta p_old ; x += alpha p_old (deferred) ; q = A0 p ; sigma = p^T W q
 template <typename R>
 struct OpCocgA {
-  static constexpr int NB = 2, NS = 1, NRED = 2;
+  static constexpr int NB = 2, NO = 1, NRED = 2;
   static constexpr bool NEEDS_W = true;
   const cx<R>* r;
   cx<R>* P0;
@@ -345,9 +346,7 @@ struct OpCocgA {
   cx<R>* p_new;
   cx<R> beta, alpha;
   bool upd;
-  struct Pre {
-    cx<R> x[3];
-  };
+  struct Pre {};
   __device__ bool skip() const { return ld_status(st) != ST_RUNNING; }
   __device__ void prepare() {
     const int k = __ldcg(&st->iter);
@@ -358,21 +357,19 @@ struct OpCocgA {
     upd = __ldcg(&st->pending) != 0;
   }
   __device__ const cx<R>* box_src(int bi) const { return bi == 0 ? r : p_old; }
-  __device__ void pre(int cell, Pre& p) const {
-    if (!upd) return;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) p.x[c] = x[c * N + cell];
-  }
+  __device__ const cx<R>* own_src(int) const { return upd ? x : nullptr; }
+  __device__ void pre(int, Pre&) const {}
+  // v = [r, p_old], ov = [x]
   __device__ cx<R> make_u(const cx<R>* v, int, int) const { return caxpy(beta, v[1], v[0]); }
-  __device__ void stash(const cx<R>* v, int, int, cx<R>* out) const { out[0] = v[1]; }
+  __device__ void convert_own(const cx<R>* v, const cx<R>* ov, int idx, int, cx<R> u, acc_t<R>*) const {
+    p_new[idx] = u;
+    if (upd) x[idx] = caxpy(alpha, v[1], ov[0]);
+  }
   __device__ void own(int cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R> W[3],
-                      const R*, const cx<R>* sv, const Pre& pr, acc_t<R>* acc) const {
+                      const R*, const Pre&, acc_t<R>* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const int idx = c * N + cell;
-      if (upd) x[idx] = caxpy(alpha, sv[c], pr.x[c]);
-      p_new[idx] = u[c];
-      q[idx] = y[c];
+      q[c * N + cell] = y[c];
       const cx<R> wp = W[c] * u[c];
       acc[0] += (double)wp.re * (double)y[c].re - (double)wp.im * (double)y[c].im;
       acc[1] += (double)wp.re * (double)y[c].im + (double)wp.im * (double)y[c].re;
@@ -506,7 +503,7 @@ struct BsBufs {
 //   x += alpha p_old + omega s ; v = A0 p ; sigma = (rh, v) ; |r|^2
 template <typename R>
 struct OpBsP {
-  static constexpr int NB = 4, NS = 2, NRED = 3;
+  static constexpr int NB = 4, NO = 1, NRED = 3;
   static constexpr bool NEEDS_W = false;
   BsBufs B;
   int N;
@@ -522,9 +519,7 @@ struct OpBsP {
   cx<R>* x;
   cx<R> alpha, omega, beta, malpha, momega;
   bool upd;
-  struct Pre {
-    cx<R> x[3];
-  };
+  struct Pre {};
   __device__ bool skip() const { return ld_status(st) != ST_RUNNING; }
   __device__ void prepare() {
     const bool odd = (__ldcg(&st->iter) & 1) != 0;
@@ -554,11 +549,8 @@ struct OpBsP {
     if (!upd && bi > 0) return nullptr;
     return bi == 0 ? ro : (bi == 1 ? vo : (bi == 2 ? t : po));
   }
-  __device__ void pre(int cell, Pre& p) const {
-    if (!upd) return;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) p.x[c] = x[c * N + cell];
-  }
+  __device__ const cx<R>* own_src(int) const { return upd ? x : nullptr; }
+  __device__ void pre(int, Pre&) const {}
   // v = [r_old, v_old, t, p_old]
   __device__ cx<R> make_u(const cx<R>* v, int, int) const {
     if (!upd) return v[0];
@@ -566,29 +558,25 @@ struct OpBsP {
     const cx<R> r = caxpy(momega, v[2], s);
     return caxpy(beta, caxpy(momega, v[1], v[3]), r);
   }
-  // stash: r_new and the owed x update alpha p_old + omega s
-  __device__ void stash(const cx<R>* v, int, int, cx<R>* out) const {
-    if (!upd) {
-      out[0] = v[0];
-      out[1] = czero<R>();
-      return;
+  // r_new, p_new and the owed x += alpha p_old + omega s need no operator: write them now
+  __device__ void convert_own(const cx<R>* v, const cx<R>* ov, int idx, int, cx<R> u, acc_t<R>* acc) const {
+    cx<R> r = v[0];
+    if (upd) {
+      const cx<R> s = caxpy(malpha, v[1], v[0]);
+      r = caxpy(momega, v[2], s);
+      x[idx] = caxpy(omega, s, caxpy(alpha, v[3], ov[0]));
     }
-    const cx<R> s = caxpy(malpha, v[1], v[0]);
-    out[0] = caxpy(momega, v[2], s);
-    out[1] = caxpy(omega, s, alpha * v[3]);
+    rn[idx] = r;
+    pn[idx] = u;
+    acc[2] += cabs2(r);
   }
-  __device__ void own(int cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R>*, const R*,
-                      const cx<R>* sv, const Pre& pr, acc_t<R>* acc) const {
+  __device__ void own(int cell, int, int, int, const cx<R>*, const cx<R> y[3], const cx<R>*, const R*,
+                      const Pre&, acc_t<R>* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int idx = c * N + cell;
-      const cx<R> r = sv[c * 2 + 0];
-      if (upd) x[idx] = pr.x[c] + sv[c * 2 + 1];
-      rn[idx] = r;
-      pn[idx] = u[c];
       vn[idx] = y[c];
       acc_cdot<R>(acc, shadow<R>(idx, seed), y[c]);
-      acc[2] += cabs2(r);
     }
   }
   __device__ void finish(const double* s) const {
@@ -611,7 +599,7 @@ struct OpBsP {
 // S pass: s = r - alpha v ; t = A0 s ; (t,s), |t|^2, (rh,t), |s|^2 ; omega, rho, beta
 template <typename R>
 struct OpBsS {
-  static constexpr int NB = 2, NS = 0, NRED = 6;
+  static constexpr int NB = 2, NO = 0, NRED = 6;
   static constexpr bool NEEDS_W = false;
   BsBufs B;
   int N;
@@ -634,9 +622,10 @@ struct OpBsS {
   __device__ const cx<R>* box_src(int bi) const { return bi == 0 ? r : v; }
   __device__ void pre(int, Pre&) const {}
   __device__ cx<R> make_u(const cx<R>* vv, int, int) const { return caxpy(malpha, vv[1], vv[0]); }
-  __device__ void stash(const cx<R>*, int, int, cx<R>*) const {}
+  __device__ const cx<R>* own_src(int) const { return nullptr; }
+  __device__ void convert_own(const cx<R>*, const cx<R>*, int, int, cx<R>, acc_t<R>*) const {}
   __device__ void own(int cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R>*, const R*,
-                      const cx<R>*, const Pre&, acc_t<R>* acc) const {
+                      const Pre&, acc_t<R>* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int idx = c * N + cell;
@@ -696,7 +685,7 @@ struct OpBsS {
 // BiCGSTAB start: r = b - A0 x0 (x0 may be zero) ; rho = (rh, r) ; |r|^2 ; status.
 template <typename R>
 struct OpBsInit {
-  static constexpr int NB = 1, NS = 0, NRED = 3;
+  static constexpr int NB = 1, NO = 0, NRED = 3;
   static constexpr bool NEEDS_W = false;
   const cx<R>* b;
   const cx<R>* x;
@@ -715,9 +704,10 @@ struct OpBsInit {
     for (int c = 0; c < 3; ++c) p.b[c] = b[c * N + cell];
   }
   __device__ cx<R> make_u(const cx<R>* v, int, int) const { return v[0]; }
-  __device__ void stash(const cx<R>*, int, int, cx<R>*) const {}
+  __device__ const cx<R>* own_src(int) const { return nullptr; }
+  __device__ void convert_own(const cx<R>*, const cx<R>*, int, int, cx<R>, acc_t<R>*) const {}
   __device__ void own(int cell, int, int, int, const cx<R>*, const cx<R> y[3], const cx<R>*, const R*,
-                      const cx<R>*, const Pre& pr, acc_t<R>* acc) const {
+                      const Pre& pr, acc_t<R>* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int idx = c * N + cell;
@@ -783,7 +773,7 @@ struct OpBsFinal {
 // (rh, r32) and |r32|^2 (the inner BiCGSTAB's starting rho and norm).
 template <typename RI>
 struct OpRefine {
-  static constexpr int NB = 1, NS = 0, NRED = 6;
+  static constexpr int NB = 1, NO = 0, NRED = 6;
   static constexpr bool NEEDS_W = true;
   const cx<double>* E_old;
   const cx<RI>* d;
@@ -812,9 +802,10 @@ struct OpRefine {
     }
     return e;
   }
-  __device__ void stash(const cx<double>*, int, int, cx<double>*) const {}
+  __device__ const cx<double>* own_src(int) const { return nullptr; }
+  __device__ void convert_own(const cx<double>*, const cx<double>*, int, int, cx<double>, double*) const {}
   __device__ void own(int cell, int, int, int, const cx<double> u[3], const cx<double> y[3],
-                      const cx<double>*, const double aW[3], const cx<double>*, const Pre& pr, double* acc) const {
+                      const cx<double>*, const double aW[3], const Pre& pr, double* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int idx = c * N + cell;
@@ -846,7 +837,7 @@ struct OpRefine {
 // matching weighted |b0|^2: the true and the symmetrised-system residuals.
 template <typename R>
 struct OpResidual {
-  static constexpr int NB = 1, NS = 0, NRED = 4;
+  static constexpr int NB = 1, NO = 0, NRED = 4;
   static constexpr bool NEEDS_W = true;
   const cx<R>* E;
   const cx<R>* J;
@@ -883,9 +874,10 @@ struct OpResidual {
     }
     return e;
   }
-  __device__ void stash(const cx<R>*, int, int, cx<R>*) const {}
+  __device__ const cx<R>* own_src(int) const { return nullptr; }
+  __device__ void convert_own(const cx<R>*, const cx<R>*, int, int, cx<R>, acc_t<R>*) const {}
   __device__ void own(int, int, int, int, const cx<R>*, const cx<R> y[3], const cx<R> W[3],
-                      const R aW[3], const cx<R>*, const Pre& pr, acc_t<R>* acc) const {
+                      const R aW[3], const Pre& pr, acc_t<R>* acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const cx<R> j = pr.j[c];
