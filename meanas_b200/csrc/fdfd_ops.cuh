@@ -296,7 +296,9 @@ struct OpCocgInit {
     return u;
   }
   __device__ const cx<R>* own_src(int) const { return nullptr; }
-  __device__ void convert_own(const cx<R>*, const cx<R>*, int, int, cx<R>, acc_t<R>*) const {}
+  __device__ void convert_own(const cx<R>*, const cx<R>*, int idx, int, cx<R> u, acc_t<R>*) const {
+    if (xnew) xnew[idx] = u;
+  }
   __device__ void own(int cell, int, int, int, const cx<R> u[3], const cx<R> y[3], const cx<R> W[3],
                       const R aW[3], const Pre& pr, acc_t<R>* acc) const {
 #pragma unroll
