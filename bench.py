@@ -76,9 +76,14 @@ def peaks() -> tuple[float, str]:
     return 6650.0, 'fallback'
 
 
-def profile_traffic(kernel: str) -> float | None:
-    """DRAM bytes per launch from the committed ncu summary (profiles/<kernel>*.md)."""
-    for f in sorted((ROOT / 'profiles').glob(f'{kernel}*.md')):
+PROFILE_TAGS = {'aniso_blocks': 'aniso160', 'dipole_core': 'dipole48', 'masked_large': 'masked320'}
+
+
+def profile_traffic(kernel: str, workload: str) -> float | None:
+    """DRAM bytes per launch of `kernel` on `workload`, from the committed ncu summary
+    profiles/<kernel>_<workload tag>.md (None when that capture does not exist)."""
+    f = ROOT / 'profiles' / f'{kernel}_{PROFILE_TAGS[workload]}.md'
+    if f.exists():
         m = re.search(r'traffic_bytes_per_launch:\s*([0-9.eE+]+)', f.read_text())
         if m:
             return float(m.group(1))
@@ -207,15 +212,25 @@ def run_ours(args) -> dict | None:
         lats = [x.elapsed_time(y) for x, y in lat]
         return max_over_ranks(total_ms, world), lats, infos
 
+    # Per-kernel CUDA-event timing inside the timed solves costs two event records per launch
+    # and disables the iteration graphs: negligible against ~0.3 ms iterations (large grids),
+    # not against 20 us ones.  Small grids time graph-launched solves for `value` and take the
+    # kernel durations from one extra profiled solve per method.
+    live = args.timed_profile == 'on' or (args.timed_profile == 'auto' and ncell >= 2_000_000)
     out = {}
     with Clocks(local) as clk:
         for method in args.methods.split(','):
-            total_ms, lats, infos = timed(method, args.steps, args.warmup, profile=True)
+            total_ms, lats, infos = timed(method, args.steps, args.warmup, profile=live)
             if args.maxiter is None:
                 assert all(i.converged and i.residual <= RTOL for i in infos), infos
-            kms = numpy.sum([i.kernel_ms for i in infos], axis=0)
-            kcnt = numpy.sum([i.kernel_count for i in infos], axis=0)
-            out[method] = dict(
+            prof_ms = total_ms
+            if not live:
+                prof_ms, _, pinfos = timed(method, 1, 0, profile=True)
+            else:
+                pinfos = infos
+            kms = numpy.sum([i.kernel_ms for i in pinfos], axis=0)
+            kcnt = numpy.sum([i.kernel_count for i in pinfos], axis=0)
+            out[method] = dict(prof_ms=prof_ms,
                 solves_per_s=world * args.steps / (total_ms / 1e3), ms_per_step=total_ms / args.steps,
                 p50_ms=float(numpy.percentile(lats, 50)), p99_ms=float(numpy.percentile(lats, 99)),
                 iterations=int(numpy.median([i.iterations for i in infos])),
@@ -265,8 +280,8 @@ def run_ours(args) -> dict | None:
         extra_bytes = (3 * real if p.mu is not None else 0) + (1 if (p.pec is not None or p.pmc is not None) else 0)
     alg = (KERNEL_BYTES_PER_CELL[dom] + extra_bytes) * ncell
     achieved = alg / (avg_ms / 1e3) / 1e9
-    traffic = profile_traffic(KERNEL_NAMES[dom])
-    share = b['kernel_ms'][dom] / (b['ms_per_step'] * args.steps)
+    traffic = profile_traffic(KERNEL_NAMES[dom], args.workload)
+    share = b['kernel_ms'][dom] / b['prof_ms']
     steps_total = args.steps
     res = {
         'metric': METRIC, 'value': round(b['solves_per_s'], 4), 'unit': 'solves/s', 'n_gpus': world,
@@ -276,9 +291,9 @@ def run_ours(args) -> dict | None:
         'data': 'synthetic (seeded)',
         'config': dict(workload_config(args.workload, p), method=best, parallelism=f'replicas x{world}'),
         'p50_ms': round(b['p50_ms'], 3), 'p99_ms': round(b['p99_ms'], 3),
-        'mixed': ({k: v for k, v in out['mixed'].items() if k not in ('kernel_ms', 'kernel_count')}
+        'mixed': ({k: v for k, v in out['mixed'].items() if k not in ('kernel_ms', 'kernel_count', 'prof_ms')}
                   if 'mixed' in out else None),
-        'fp64': ({k: v for k, v in out['cocg'].items() if k not in ('kernel_ms', 'kernel_count')}
+        'fp64': ({k: v for k, v in out['cocg'].items() if k not in ('kernel_ms', 'kernel_count', 'prof_ms')}
                  if 'cocg' in out else None),
         'mixed_over_fp64': (round(out['mixed']['solves_per_s'] / out['cocg']['solves_per_s'], 3)
                             if 'mixed' in out and 'cocg' in out else None),
@@ -286,7 +301,10 @@ def run_ours(args) -> dict | None:
                      'peak': peak, 'unit': 'GB/s', 'frac': round(achieved / peak, 4),
                      'peak_kind': peak_kind, 'traffic': traffic,
                      'algorithmic_bytes_per_launch': alg, 'avg_launch_ms': round(avg_ms, 5),
-                     'share_of_step': round(share, 3)},
+                     'share_of_step': round(share, 3),
+                     'timing': ('CUDA events around every launch of the timed solves' if live else
+                                'CUDA events around every launch of one profiled solve after the '
+                                'graph-launched timed solves')},
         'gpu_launches': int(b['launches']),
         'tiling': {k: {'xchunk': v[0], 'us_per_iteration': round(v[1], 1)} for k, v in tuned.items()},
         'clocks': clocks,
@@ -495,6 +513,8 @@ def main():
     ap.add_argument('--kernel-iters', type=int, default=0,
                     help='profiling mode: run this many iterations of each solver (no convergence, no JSON)')
     ap.add_argument('--shape', type=int, nargs=3, default=None, help='profiling mode grid shape')
+    ap.add_argument('--timed-profile', choices=['auto', 'on', 'off'], default='auto',
+                    help='per-launch CUDA events inside the timed solves (auto: grids of >= 2M cells)')
     ap.add_argument('--maxiter', type=int, default=None,
                     help='cap the Krylov iterations of each timed solve (measurement runs; reports the status)')
     ap.add_argument('--gradient-check', action='store_true', help='adjoint gradient vs finite differences')
