@@ -433,7 +433,7 @@ def gradient_check(args) -> dict:
     cells = numpy.flatnonzero(p.extra['design_mask'].ravel())
     rng = numpy.random.default_rng(0)
     h = 1e-4
-    errs = []
+    errs, fds, ads = [], [], []
     with torch.no_grad():
         for cell in rng.choice(cells, args.fd_cells, replace=False):
             idx = [cell, n + cell, 2 * n + cell]
@@ -444,11 +444,21 @@ def gradient_check(args) -> dict:
             fd = (loss(ep) - loss(em)).item() / (2 * h)
             ad = float(g[idx].sum())
             errs.append(abs(fd - ad) / max(abs(fd), 1e-300))
+            fds.append(fd)
+            ads.append(ad)
+    fds, ads = numpy.array(fds), numpy.array(ads)
+    # Per-cell relative errors are dominated by finite-difference noise where the gradient is
+    # tiny (the solves' 1e-12 residual divided by 2h); the normwise error over the sampled
+    # cells and the per-cell error on cells carrying >= 1e-3 of the largest |dL/deps| are not.
+    big = numpy.abs(fds) >= 1e-3 * numpy.abs(fds).max()
     design_g = g[numpy.tile(p.extra['design_mask'].ravel(), 3)]
     return {'metric': 'adjoint gradient dL/deps vs central finite differences', 'workload':
             'adjoint_design 96x96x64, 10-cell SC-PML, omega=2pi/26, 40x40x8 design, L=sum|E|^2 at x=76',
             'fd_cells': args.fd_cells, 'h': h, 'solve_rtol': 1e-12, 'max_rel_err': max(errs),
-            'median_rel_err': float(numpy.median(errs)), 'gradient_seconds': round(t_grad, 3),
+            'median_rel_err': float(numpy.median(errs)),
+            'normwise_rel_err': float(numpy.linalg.norm(fds - ads) / numpy.linalg.norm(fds)),
+            'max_rel_err_significant_cells': float(numpy.max(numpy.array(errs)[big])),
+            'significant_cells': int(big.sum()), 'gradient_seconds': round(t_grad, 3),
             'loss': L.item(), 'grad_norm_design': float(numpy.linalg.norm(design_g))}
 
 

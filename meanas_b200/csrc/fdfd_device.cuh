@@ -23,6 +23,8 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <type_traits>
+#include <utility>
 
 namespace fdfd {
 
@@ -155,38 +157,52 @@ struct RedBuf {
   unsigned int* ticket;    // zero between launches (reset by the last CTA)
 };
 
-template <int NT>
-__device__ __forceinline__ double block_sum(double v, double* sh) {
-  // warp tree, then a fixed-order tree over warps
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  const int lane = threadIdx.x & 31, warp = (threadIdx.x + threadIdx.y * blockDim.x) >> 5;
-  const int ln = (threadIdx.x + threadIdx.y * blockDim.x) & 31;
-  (void)lane;
-  __syncthreads();
-  if (ln == 0) sh[warp] = v;
+// Sum NRED values over the CTA at once: warp trees for all values, one pass through
+// shared memory (sh[warp][r]), then thread r < NRED sums value r over the warps in a
+// fixed order and returns it (other threads return 0).
+template <int NT, int NRED>
+__device__ __forceinline__ double block_sum_n(double (&v)[NRED], double* sh) {
+  constexpr int NW = (NT + 31) / 32;
+  static_assert(NW * NRED <= 64, "reduction scratch is 64 doubles");
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int r = 0; r < NRED; ++r) v[r] += __shfl_down_sync(0xffffffffu, v[r], o);
+  }
+  __syncthreads();  // sh free (earlier readers done)
+  if ((tid & 31) == 0) {
+#pragma unroll
+    for (int r = 0; r < NRED; ++r) sh[(tid >> 5) * NRED + r] = v[r];
+  }
   __syncthreads();
   double s = 0.0;
-  if (warp == 0) {
-    constexpr int NW = (NT + 31) / 32;
-    s = (ln < NW) ? sh[ln] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (tid < NRED) {
+#pragma unroll
+    for (int w = 0; w < NW; ++w) s += sh[w * NRED + tid];
   }
-  return s;  // valid in thread 0
+  return s;
 }
 
 // Reduce NRED per-thread accumulators across the grid; returns true in the one
-// thread (thread 0 of the last CTA) that holds the final sums in `out`.
+// thread (thread 0 of the last CTA) that holds the final sums in `out`.  Partials are
+// [CTA][NRED]; the last CTA reads them with independent loads (no per-value passes), so
+// the serial tail after the last CTA's own work is about two L2 round trips.
 template <int NT, int NRED, typename A>
 __device__ bool grid_reduce(const A (&acc)[NRED], RedBuf rb, double* sh, double* out) {
   const int tid = threadIdx.x + threadIdx.y * blockDim.x;
   __shared__ bool s_last;
+  double v[NRED];
 #pragma unroll
-  for (int r = 0; r < NRED; ++r) {
-    double s = block_sum<NT>((double)acc[r], sh);
-    if (tid == 0) rb.partials[(size_t)blockIdx.x * NRED + r] = s;
-  }
-  if (tid == 0) {
+  for (int r = 0; r < NRED; ++r) v[r] = (double)acc[r];
+  const double part = block_sum_n<NT, NRED>(v, sh);
+  if (tid < NRED) {
+    rb.partials[(size_t)blockIdx.x * NRED + tid] = part;
     __threadfence();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();  // cumulative: the partials written before the barrier are visible first
     unsigned int t = atomicAdd(rb.ticket, 1u);
     s_last = (t == gridDim.x - 1);
   }
@@ -194,15 +210,54 @@ __device__ bool grid_reduce(const A (&acc)[NRED], RedBuf rb, double* sh, double*
   if (!s_last) return false;
   __threadfence();
   const unsigned int nb = gridDim.x;
+  double s[NRED];
 #pragma unroll
-  for (int r = 0; r < NRED; ++r) {
-    double s = 0.0;
-    for (unsigned int b = tid; b < nb; b += NT) s += __ldcg(&rb.partials[(size_t)b * NRED + r]);
-    s = block_sum<NT>(s, sh);
-    if (tid == 0) out[r] = s;
+  for (int r = 0; r < NRED; ++r) s[r] = 0.0;
+#pragma unroll 4
+  for (unsigned int b = tid; b < nb; b += NT) {
+#pragma unroll
+    for (int r = 0; r < NRED; ++r) s[r] += __ldcg(&rb.partials[(size_t)b * NRED + r]);
   }
-  if (tid == 0) *rb.ticket = 0u;
+  const double tot = block_sum_n<NT, NRED>(s, sh);
+  __syncthreads();  // sh reads of block_sum_n done
+  if (tid < NRED) sh[tid] = tot;
+  __syncthreads();
+  if (tid == 0) {
+#pragma unroll
+    for (int r = 0; r < NRED; ++r) out[r] = sh[r];
+    *rb.ticket = 0u;
+  }
   return tid == 0;
+}
+
+// Ops that carry solver state (a member `st` pointing to it) run finish() on a copy:
+// the last CTA's thread 0 loads the whole state with independent loads, runs the scalar
+// recurrences on the copy and stores it back, instead of a chain of dependent L2 round
+// trips through the global struct.  No other thread reads the state at that point (the
+// other CTAs have passed the ticket; the host reads it after the kernel).
+template <class Op, class = void>
+struct HasState : std::false_type {};
+template <class Op>
+struct HasState<Op, std::void_t<decltype(std::declval<Op&>().st)>> : std::true_type {};
+
+// Out of line, so the state copy's registers are not reserved by the whole kernel.
+template <class Op>
+__device__ __noinline__ void finish_on_copy(Op o, const double* sums) {
+  using St = std::remove_pointer_t<decltype(o.st)>;
+  St* const g = o.st;
+  St loc = *g;
+  o.st = &loc;
+  o.finish(sums);
+  *g = loc;
+}
+
+template <class Op>
+__device__ __forceinline__ void run_finish(const Op& o, const double* sums) {
+  if constexpr (HasState<Op>::value) {
+    finish_on_copy(o, sums);
+  } else {
+    o.finish(sums);
+  }
 }
 
 // ---------------------------------------------------------------- stencil engine
@@ -462,14 +517,12 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
 
   // ---- prologue: planes x0-1 and x0 into U, H on plane x0-1 (own cells: Hy, Hz)
   const int ip = wrapi(x0 - 1, g.X);
+  // (own slots only until the barrier: the barrier publishes Xt, U[0] and U[1])
   issue(ip);
   cp_async_wait_all();
-  __syncthreads();
   convert(0, ip, false);
-  __syncthreads();
   issue(x0);
   cp_async_wait_all();
-  __syncthreads();
   convert(1, x0, true);
   __syncthreads();
   // plane x0+1 starts landing while the prologue H is computed
@@ -496,10 +549,12 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
 #pragma unroll
       for (int c = 0; c < 3; ++c) e3[c] = g.eps[c * N + cell];
     }
-    cp_async_wait_all();   // plane i+1 landed
-    __syncthreads();       // ... for everyone; U[nxt] (plane i-1) and Hs no longer read
+    // Plane i+1's raw inputs landed.  No barrier is needed here: every thread copies and
+    // converts only its own Sbox/Sown slots, U[nxt] (plane i-1) was last read before the
+    // previous step's Hs barrier, and Hs is rewritten only after the barrier below.
+    cp_async_wait_all();
     convert(nxt, in1, i + 1 < x1);
-    __syncthreads();       // U[nxt] = u(i+1) ready; Sbox free
+    __syncthreads();       // U[nxt] = u(i+1) ready for the neighbours' differences
     if (i + 1 < x1) issue(in1 + 1 == g.X ? 0 : in1 + 1);
     const cx<R>* xe = Xt + (i - x0 + 1) * S::XT_STRIDE;
     const cx<R> idxe_i = xe[0], idxh_i = xe[1];
@@ -565,13 +620,16 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
 
   if constexpr (Op::NRED > 0) {
     double sums[Op::NRED];
-    if (grid_reduce<NT, Op::NRED>(acc, rb, shred, sums)) o.finish(sums);
+    if (grid_reduce<NT, Op::NRED>(acc, rb, shred, sums)) run_finish(o, sums);
   }
 }
 
 // ---------------------------------------------------------------- pointwise engine
-// Same CTA geometry without the stencil: own cells of the tile over the x chunk.
-//   void point(int cell, int i, int j, int k, const cx<R> W[3], double* acc);
+// Own cells only, no stencil.  Work units are (x plane, y/z tile) pairs, tiles fastest;
+// the grid is sized to the GPU's resident CTA slots and CTA b takes units b, b + grid,
+// b + 2 grid, ...  The assignment is fixed (the reductions stay deterministic) and every
+// SM streams to the end instead of idling through a partial last wave.
+//   void point(int cell, int i, int j, int k, const cx<R> W[3], const R aW[3], A* acc);
 template <typename R, int TZ, int TY, class Op>
 __global__ void __launch_bounds__(TZ * TY) k_point(const Geo<R> g, Op op, RedBuf rb) {
   constexpr int NT = TZ * TY;
@@ -580,31 +638,31 @@ __global__ void __launch_bounds__(TZ * TY) k_point(const Geo<R> g, Op op, RedBuf
   Op o = op;
   o.prepare();
   const int tz = threadIdx.x, ty = threadIdx.y;
-  int b = blockIdx.x;
-  const int tzb = b % g.ntz; b /= g.ntz;
-  const int tyb = b % g.nty;
-  const int xcb = b / g.nty;
-  const int j = tyb * TY + ty, k = tzb * TZ + tz;
-  const int x0 = xcb * g.XC, x1 = min(g.X, x0 + g.XC);
-  const bool active = (j < g.Y) && (k < g.Z);
-  const int YZ = (int)g.Y * g.Z;
-  WeightYZ<R> wyz;
-  if (Op::NEEDS_W) wyz.init(g, min(j, g.Y - 1), min(k, g.Z - 1));
+  const int ntiles = g.ntz * g.nty;
+  const int units = ntiles * g.X;
+  const int YZ = g.Y * g.Z;
   using A = typename AccT<R>::type;
   A acc[Op::NRED > 0 ? Op::NRED : 1];
 #pragma unroll
   for (int r = 0; r < (Op::NRED > 0 ? Op::NRED : 1); ++r) acc[r] = A(0);
-  if (active) {
-#pragma unroll 2
-    for (int i = x0; i < x1; ++i) {
+  for (int u = blockIdx.x; u < units; u += gridDim.x) {
+    const int i = u / ntiles, t = u - i * ntiles;
+    const int tyb = t / g.ntz, tzb = t - tyb * g.ntz;
+    const int j = tyb * TY + ty, k = tzb * TZ + tz;
+    if (j < g.Y && k < g.Z) {
       cx<R> W[3];
       R aW[3];
-      if (Op::NEEDS_W) wyz.at(g.dxe[0][i], g.dxh[0][i], g.adxe[0][i], g.adxh[0][i], W, aW);
-      o.point((int)i * YZ + (int)j * g.Z + k, i, j, k, W, aW, acc);
+      if (Op::NEEDS_W) {
+        WeightYZ<R> wyz;
+        wyz.init(g, j, k);
+        wyz.at(g.dxe[0][i], g.dxh[0][i], g.adxe[0][i], g.adxh[0][i], W, aW);
+      }
+      o.point(i * YZ + j * g.Z + k, i, j, k, W, aW, acc);
     }
   }
   if constexpr (Op::NRED > 0) {
     double sums[Op::NRED];
+    // (finish runs on the global state here: a state copy would cost this kernel occupancy)
     if (grid_reduce<NT, Op::NRED>(acc, rb, shred, sums)) o.finish(sums);
   }
 }

@@ -268,15 +268,30 @@ static int launch_stencil(fdfd_plan* P, const Geo<R>& g0, int precision, const O
   return 0;
 }
 
+template <typename K>
+static int occupancy(K kern, int threads) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, 0) != cudaSuccess || n < 1) n = 1;
+  return n;
+}
+
 template <typename R, class Op>
 static int launch_point(fdfd_plan* P, const Geo<R>& g0, int precision, const Op& op, RedBuf rb,
                         cudaStream_t s) {
   const Tiling t = make_tiling(P, precision);
   const Geo<R> g = geo_with(g0, t);
+  const long long units = (long long)t.ntz * t.nty * P->X;
+  // one CTA per resident slot (occupancy of this kernel, queried once)
   if (P->flat) {
-    k_point<R, 1, FLAT_TY, Op><<<(unsigned)t.nblocks, dim3(1, FLAT_TY), 0, s>>>(g, op, rb);
+    auto kern = k_point<R, 1, FLAT_TY, Op>;
+    static const int occ = occupancy(kern, FLAT_TY);
+    const unsigned grid = (unsigned)std::min(units, (long long)occ * P->nsm);
+    kern<<<grid, dim3(1, FLAT_TY), 0, s>>>(g, op, rb);
   } else {
-    k_point<R, TZ3, TY3, Op><<<(unsigned)t.nblocks, dim3(TZ3, TY3), 0, s>>>(g, op, rb);
+    auto kern = k_point<R, TZ3, TY3, Op>;
+    static const int occ = occupancy(kern, TZ3 * TY3);
+    const unsigned grid = (unsigned)std::min(units, (long long)occ * P->nsm);
+    kern<<<grid, dim3(TZ3, TY3), 0, s>>>(g, op, rb);
   }
   P->launches++;
   CKL();
