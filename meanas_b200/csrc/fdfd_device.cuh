@@ -535,6 +535,10 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
     hy_prev = hy;
     hz_prev = hz;
   }
+  // The first step converts plane x0+1 into U[0]: every thread must be done reading
+  // U[0] (plane x0-1) for the prologue H.  (Inside the loop the previous step's Hs
+  // barrier gives this ordering.)
+  __syncthreads();
   int cur = 1;
   for (int i = x0; i < x1; ++i) {
     const int nxt = cur ^ 1;
