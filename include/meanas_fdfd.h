@@ -173,6 +173,20 @@ int fdfd_residual(fdfd_plan* plan, const void* E, const void* J, double out[4], 
  * generic(adjoint=True) (meanas/fdfd/solvers.py:119-137); grad: float64[3N]. */
 int fdfd_eps_gradient(fdfd_plan* plan, const void* E, const void* E_adj, double* grad, void* stream);
 
+/* fdfd_e2h flags */
+#define FDFD_E2H_CONJ 1 /* S = E x conj(H) instead of E x H */
+#define FDFD_E2H_H_IN 2 /* H is an input: only S is computed, from E and the caller's H */
+
+/* The step after the solve: H = e2h(omega, dxes, mu, pmc) @ E
+ * (meanas/fdfd/operators.py:253-282: pm diag(1/mu) ce(E) / (-i omega)) into H, and when
+ * S is not NULL the Yee-grid cross product S = E x H (functional.poynting_e_cross_h,
+ * meanas/fdfd/functional.py:187-221) or, with FDFD_E2H_CONJ, S = E x conj(H) (the
+ * poynting_e_cross(E) @ H.conj() of meanas/fdfd/operators.py:310-336 that
+ * meanas/test/test_fdfd.py:38-40 forms; Re(S)/2 is the time-averaged Poynting vector).
+ * With FDFD_E2H_H_IN, H is read instead of computed.  E, H, S: complex128 [3N] device
+ * arrays; H may be NULL when only S is wanted. */
+int fdfd_e2h(fdfd_plan* plan, const void* E, void* H, void* S, int32_t flags, void* stream);
+
 /* fdfd_residual without a workspace, for callers that cannot allocate device memory
  * (an exhausted or frozen allocator, or a host program that owns every device buffer
  * and can pass only inputs and outputs).  No counterpart in the reference.

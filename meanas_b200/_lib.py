@@ -91,7 +91,12 @@ EXPORTS = {
                                 C.c_size_t, C.c_void_p]),
     'fdfd_eps_gradient': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     'fdfd_residual_static': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_void_p]),
+    'fdfd_e2h': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
 }
+
+# fdfd_e2h flags (include/meanas_fdfd.h)
+E2H_CONJ = 1
+E2H_H_IN = 2
 
 _lib: C.CDLL | None = None
 

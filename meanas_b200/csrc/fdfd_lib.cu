@@ -1037,6 +1037,40 @@ extern "C" int fdfd_eps_gradient(fdfd_plan* P, const void* E, const void* E_adj,
   return launch_point<double>(P, P->g64, 0, op, RedBuf{nullptr, nullptr}, s);
 }
 
+// ------------------------------------------------------------------ E -> H, Poynting
+extern "C" int fdfd_e2h(fdfd_plan* P, const void* E, void* H, void* S, int32_t flags, void* stream) {
+  if (!P || !E) return set_err(FDFD_ERR_ARG, "fdfd_e2h: NULL plan or E");
+  if (!H && !S) return set_err(FDFD_ERR_ARG, "fdfd_e2h: both outputs are NULL");
+  if (flags & ~(FDFD_E2H_CONJ | FDFD_E2H_H_IN)) return set_err(FDFD_ERR_ARG, "fdfd_e2h: unknown flags %d", flags);
+  const int conj_h = (flags & FDFD_E2H_CONJ) != 0, h_in = (flags & FDFD_E2H_H_IN) != 0;
+  if (h_in && (!H || !S)) return set_err(FDFD_ERR_ARG, "fdfd_e2h: FDFD_E2H_H_IN needs both H and S");
+  const double m2 = P->om_re * P->om_re + P->om_im * P->om_im;
+  if (!(m2 > 0.0)) return set_err(FDFD_ERR_ARG, "fdfd_e2h: omega is zero");
+  cudaStream_t s = (cudaStream_t)stream;
+  P->launches = 0;
+  const cx<double> inv_miw = mkc<double>(P->om_im / m2, P->om_re / m2);  // 1 / (-i omega)
+  const Tiling t = make_tiling(P, 0);
+  const Geo<double> g = geo_with(P->g64, t);
+  const long long units = (long long)t.ntz * t.nty * P->X;
+  const cx<double>* e = (const cx<double>*)E;
+  cx<double>* h = (cx<double>*)H;
+  cx<double>* sv = (cx<double>*)S;
+  if (P->flat) {
+    auto kern = k_e2h<1, FLAT_TY>;
+    static const int occ = occupancy(kern, FLAT_TY);
+    kern<<<(unsigned)std::min(units, (long long)occ * P->nsm), dim3(1, FLAT_TY), 0, s>>>(g, e, h, sv, inv_miw,
+                                                                                       conj_h, h_in);
+  } else {
+    auto kern = k_e2h<TZ3, TY3>;
+    static const int occ = occupancy(kern, TZ3 * TY3);
+    kern<<<(unsigned)std::min(units, (long long)occ * P->nsm), dim3(TZ3, TY3), 0, s>>>(g, e, h, sv, inv_miw,
+                                                                                        conj_h, h_in);
+  }
+  P->launches++;
+  CKL();
+  return 0;
+}
+
 // ------------------------------------------------------------------ allocation-free residual
 // For callers that cannot allocate device memory at all (for example code running
 // under an allocator that is already exhausted or frozen, or a host application

@@ -954,4 +954,70 @@ struct OpCopy {
   __device__ void finish(const double*) const {}
 };
 
+// ------------------------------------------------------------------ E -> H, E x H
+// The step after the solve: H = pm mu^-1 ce(E) / (-i omega) (the sparse e2h of
+// meanas/fdfd/operators.py:253-282) and, when S is set, S = E x H' with H' = conj(H)
+// (conj_h, the product meanas/test/test_fdfd.py:38-40 forms) or H (H itself the
+// caller's when h_in: functional.poynting_e_cross_h(dxes)(E, H)), on the Yee grid of
+// meanas/fdfd/functional.py:187-221: E components weighted by dx_e and taken one cell
+// up along the cross axis, H components weighted by dx_h.  One thread per cell over
+// (x plane, y/z tile) units like the pointwise engine; E's +1 neighbours come through
+// L1/L2, so HBM sees E once and H, S once each.
+template <int TZ, int TY>
+__global__ void __launch_bounds__(TZ * TY) k_e2h(const Geo<double> g, const cx<double>* __restrict__ E,
+                                                 cx<double>* __restrict__ H, cx<double>* __restrict__ S,
+                                                 cx<double> inv_miw, int conj_h, int h_in) {
+  using C = cx<double>;
+  const int ntiles = g.ntz * g.nty, units = ntiles * g.X, YZ = g.Y * g.Z, N = g.N;
+  for (int u = blockIdx.x; u < units; u += gridDim.x) {
+    const int i = u / ntiles, t = u - i * ntiles;
+    const int tyb = t / g.ntz, tzb = t - tyb * g.ntz;
+    const int j = tyb * TY + threadIdx.y, k = tzb * TZ + threadIdx.x;
+    if (j >= g.Y || k >= g.Z) continue;
+    const int i1 = i + 1 == g.X ? 0 : i + 1, j1 = j + 1 == g.Y ? 0 : j + 1, k1 = k + 1 == g.Z ? 0 : k + 1;
+    const int c0 = i * YZ + j * g.Z + k;
+    const int cx1 = i1 * YZ + j * g.Z + k, cy1 = i * YZ + j1 * g.Z + k, cz1 = i * YZ + j * g.Z + k1;
+    const C ex = E[c0], ey = E[N + c0], ez = E[2 * N + c0];
+    const C ey_x1 = E[N + cx1], ez_x1 = E[2 * N + cx1];
+    const C ex_y1 = E[cy1], ez_y1 = E[2 * N + cy1];
+    const C ex_z1 = E[cz1], ey_z1 = E[N + cz1];
+    C hx, hy, hz;
+    if (h_in) {  // S from the caller's H
+      hx = H[c0];
+      hy = H[N + c0];
+      hz = H[2 * N + c0];
+    } else {
+      const C ix = g.idxe[0][i], iy = g.idxe[1][j], iz = g.idxe[2][k];
+      hx = ((ez_y1 - ez) * iy - (ey_z1 - ey) * iz) * inv_miw;
+      hy = ((ex_z1 - ex) * iz - (ez_x1 - ez) * ix) * inv_miw;
+      hz = ((ey_x1 - ey) * ix - (ex_y1 - ex) * iy) * inv_miw;
+      if (g.muinv) {
+        hx = g.muinv[c0] * hx;
+        hy = g.muinv[N + c0] * hy;
+        hz = g.muinv[2 * N + c0] * hz;
+      }
+      if (g.mask) {
+        const uint8_t m = g.mask[c0];
+        if (m & 8u) hx = czero<double>();
+        if (m & 16u) hy = czero<double>();
+        if (m & 32u) hz = czero<double>();
+      }
+    }
+    if (H && !h_in) {
+      H[c0] = hx;
+      H[N + c0] = hy;
+      H[2 * N + c0] = hz;
+    }
+    if (S) {
+      const C wx = (conj_h ? cconj(hx) : hx) * g.dxh[0][i];
+      const C wy = (conj_h ? cconj(hy) : hy) * g.dxh[1][j];
+      const C wz = (conj_h ? cconj(hz) : hz) * g.dxh[2][k];
+      const C dex = g.dxe[0][i], dey = g.dxe[1][j], dez = g.dxe[2][k];
+      S[c0] = (ey_x1 * dey) * wz - (ez_x1 * dez) * wy;
+      S[N + c0] = (ez_y1 * dez) * wx - (ex_y1 * dex) * wz;
+      S[2 * N + c0] = (ex_z1 * dex) * wy - (ey_z1 * dey) * wx;
+    }
+  }
+}
+
 }  // namespace fdfd

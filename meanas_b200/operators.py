@@ -221,6 +221,34 @@ class GridOperator:
                                                   _stream_handle()))
         return g
 
+    # ------------------------------------------------------------------ after the solve
+    def e2h(self, E, out: torch.Tensor | None = None) -> torch.Tensor:
+        """``H = pm diag(1/mu) ce(E) / (-i omega)``: the reference's sparse
+        ``operators.e2h(omega, dxes, mu, pmc) @ E`` (``meanas/fdfd/operators.py:253-282``)."""
+        Et = as_device(E, torch.complex128, self.device, self.n, 'E')
+        H = out if out is not None else torch.empty_like(Et)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.fdfd_e2h(self.plan, Et.data_ptr(), H.data_ptr(), None, 0, _stream_handle()))
+        return H
+
+    def poynting(self, E, H=None, *, conj: bool = True) -> tuple[torch.Tensor, torch.Tensor]:
+        """``(S, H)`` with ``S = E x conj(H)`` (``conj=False``: ``E x H``) on the Yee grid of
+        ``meanas/fdfd/functional.py:187-221`` -- the ``poynting_e_cross(E) @ H.conj()`` of
+        ``meanas/test/test_fdfd.py:38-40``; ``Re(S)/2`` is the time-averaged Poynting vector.
+        With ``H=None``, H is ``e2h(E)`` and both come from one pass over E."""
+        Et = as_device(E, torch.complex128, self.device, self.n, 'E')
+        S = torch.empty_like(Et)
+        flags = _lib.E2H_CONJ if conj else 0
+        if H is None:
+            Ht = torch.empty_like(Et)
+        else:
+            Ht = as_device(H, torch.complex128, self.device, self.n, 'H')
+            flags |= _lib.E2H_H_IN
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.fdfd_e2h(self.plan, Et.data_ptr(), Ht.data_ptr(), S.data_ptr(), flags,
+                                         _stream_handle()))
+        return S, Ht
+
     # ------------------------------------------------------------------ solve
     def solve_opts(self, *, method: str = 'cocg', rtol: float = 1e-8, atol: float = 0.0,
                    maxiter: int | None = None, criterion: str = 'true', adjoint: bool = False,

@@ -27,6 +27,12 @@ What each function restates:
   pins ``scipy~=1.14`` in ``pyproject.toml:44``, ``uv.lock`` locks 1.16.3); it
   is called, not restated.  The adjoint branch (``:119-137``) is written with
   explicit conjugate transposes, since ``csr_array.H`` is gone in SciPy >= 1.14.
+* ``e2h``            ``H = pm diag(1/mu) ce(E) / (-i omega)``, the sparse
+  ``meanas/fdfd/operators.py:253-282`` (its functional twin
+  ``meanas/fdfd/functional.py:89-117`` has no PMC argument).
+* ``poynting_e_cross_h``  ``E x H`` with the one-cell shift of E and the cell-width
+  weights of ``meanas/fdfd/functional.py:187-221`` (the same product as
+  ``operators.poynting_e_cross(E) @ H``, ``meanas/fdfd/operators.py:310-336``).
 * ``cocg``           complex-symmetric CG in the E-space with the ``p^2``-weighted
   bilinear form: algebraically the COCG iteration on ``Pl A0 Pr`` (the system
   ``generic()`` builds) rewritten with ``x = Pl E``; the GPU solver runs the same
@@ -93,6 +99,36 @@ def e_full_apply(omega, dxes, epsilon, E, mu=None, pec=None, pmc=None) -> NDArra
     if pec is not None:
         y = y * numpy.where(numpy.asarray(pec).reshape(f3), 0, 1)
     return y.ravel()
+
+
+def e2h(omega, dxes, E, mu=None, pmc=None) -> NDArray:
+    """``H = pm diag(1/mu) ce(E) / (-i omega)`` for 1D C-order vectors, complex128 (3XYZ,)
+    (``meanas/fdfd/operators.py:253-282``)."""
+    shape = _shape_of(dxes)
+    f3 = (3, *shape)
+    h = curl_forward(dxes[0], numpy.asarray(E, dtype=complex).reshape(f3)) / (-1j * omega)
+    if mu is not None:
+        h = h / numpy.asarray(mu).reshape(f3)
+    if pmc is not None:
+        h = h * numpy.where(numpy.asarray(pmc).reshape(f3), 0, 1)
+    return h.ravel()
+
+
+def poynting_e_cross_h(dxes, E, H) -> NDArray:
+    """``E x H`` on the Yee grid (``meanas/fdfd/functional.py:187-221``): components of E
+    weighted by ``dx_e``, of H by ``dx_h``, E shifted by one cell along the cross axis.
+    Pass ``H.conj()`` for the complex Poynting vector; complex128 (3XYZ,)."""
+    shape = _shape_of(dxes)
+    f3 = (3, *shape)
+    e = numpy.asarray(E, dtype=complex).reshape(f3)
+    h = numpy.asarray(H, dtype=complex).reshape(f3)
+    ex, ey, ez = (e[a] * _bcast(dxes[0][a], a) for a in range(3))
+    hx, hy, hz = (h[a] * _bcast(dxes[1][a], a) for a in range(3))
+    s = numpy.empty_like(e)
+    s[0] = numpy.roll(ey, -1, axis=0) * hz - numpy.roll(ez, -1, axis=0) * hy
+    s[1] = numpy.roll(ez, -1, axis=1) * hx - numpy.roll(ex, -1, axis=1) * hz
+    s[2] = numpy.roll(ex, -1, axis=2) * hy - numpy.roll(ey, -1, axis=2) * hx
+    return s.ravel()
 
 
 def precond_p2(dxes) -> NDArray:

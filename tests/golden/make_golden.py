@@ -16,6 +16,10 @@ the only place that reads it.  Outputs:
                     atol 1e-15), the 1D PML cases of ``meanas/test/test_fdfd_pml.py``
                     (their unidirectional sources included), and 3D PML problems
                     with mu, PEC and PMC, forward and adjoint.
+* ``e2h.npz``       ``operators.e2h @ x`` (mu, PMC) and the Poynting products
+                    ``operators.poynting_e_cross(x) @ conj(H)`` and
+                    ``functional.poynting_e_cross_h(dxes)(x, conj(H))`` on random
+                    small problems.
 * ``dipole48.npz``  reference ``generic()`` on the 48^3 dipole-in-core problem
                     (rtol 1e-8, scipy QMR): field stored as complex64.
 """
@@ -32,7 +36,7 @@ sys.path.insert(0, REF)
 sys.path.insert(0, str(Path(__file__).resolve().parents[2]))
 
 import scipy.sparse  # noqa: E402
-from meanas.fdfd import operators, scpml, solvers, waveguide_3d  # noqa: E402
+from meanas.fdfd import functional, operators, scpml, solvers, waveguide_3d  # noqa: E402
 from meanas.fdmath import vec, unvec  # noqa: E402
 
 # generic(adjoint=True) uses csr_array.H, which SciPy >= 1.14 removed.
@@ -118,6 +122,44 @@ def gen_operator() -> None:
         out[p + 'pl'] = Pl.diagonal()
     out['n'] = numpy.array(len(cases))
     numpy.savez_compressed(OUT / 'operator.npz', **out)
+
+
+def gen_e2h() -> None:
+    rng = numpy.random.default_rng(77)
+    out = {}
+    cases = [((6, 5, 4), True, True, 2),
+             ((7, 6, 1), False, True, 2),
+             ((1, 6, 7), True, False, 0),
+             ((9, 8, 7), False, False, 3),
+             ((21, 9, 34), True, True, 4),
+             ((4, 37, 1), True, True, 1)]
+    for n, (shape, use_mu, use_pmc, th) in enumerate(cases):
+        om = complex(2 * numpy.pi / rng.uniform(6, 12), 0.0) if n != 3 else complex(0.9, 0.05)
+        dxes = [[rng.uniform(0.8, 1.3, s) for s in shape] for _ in range(2)]
+        sf = scpml.prepare_s_function(ln_R=-16, m=3.5)
+        for ax in range(3):
+            if shape[ax] > 2 * th + 1 and th > 0:
+                for pol in (-1, 1):
+                    dxes = scpml.stretch_with_scpml(dxes, axis=ax, polarity=pol, omega=om.real,
+                                                    thickness=th, s_function=sf)
+        N3 = 3 * int(numpy.prod(shape))
+        mu = rng.uniform(1, 1.5, N3) if use_mu else None
+        pmc = (rng.random(N3) < 0.05).astype(float) if use_pmc else None
+        x = rng.standard_normal(N3) + 1j * rng.standard_normal(N3)
+        H = operators.e2h(om, dxes, mu, pmc) @ x
+        p = f'c{n}_'
+        out[p + 'shape'] = numpy.array(shape)
+        out[p + 'omega'] = numpy.array(om)
+        pack_dxes(p, dxes, out)
+        for name, arr in (('mu', mu), ('pmc', pmc)):
+            if arr is not None:
+                out[p + name] = arr
+        out[p + 'x'] = x
+        out[p + 'H'] = H
+        out[p + 'S_op'] = operators.poynting_e_cross(x, dxes) @ H.conj()
+        out[p + 'S_fn'] = vec(functional.poynting_e_cross_h(dxes)(unvec(x, shape), unvec(H.conj(), shape)))
+    out['n'] = numpy.array(len(cases))
+    numpy.savez_compressed(OUT / 'e2h.npz', **out)
 
 
 def gen_solve() -> None:
@@ -258,7 +300,7 @@ def gen_dipole48() -> None:
 
 
 if __name__ == '__main__':
-    which = sys.argv[2:] or ['scpml', 'operator', 'solve', 'dipole48']
+    which = sys.argv[2:] or ['scpml', 'operator', 'e2h', 'solve', 'dipole48']
     for w in which:
         t = time.perf_counter()
         globals()[f'gen_{w}']()

@@ -10,6 +10,7 @@ from meanas_b200 import scpml
 
 OPS = golden_cases('operator')
 SOLVES = golden_cases('solve')
+E2H = golden_cases('e2h')
 
 
 def _opt(c, k):
@@ -22,6 +23,16 @@ def test_oracle_apply_matches_reference(c):
     y = O.e_full_apply(om, c['dxes'], c['eps'], c['x'], _opt(c, 'mu'), _opt(c, 'pec'), _opt(c, 'pmc'))
     ref = c['A0x']
     assert numpy.linalg.norm(y - ref) <= 1e-14 * numpy.linalg.norm(ref)
+
+
+@pytest.mark.parametrize('c', E2H, ids=lambda c: f"e2h{c['index']}-{tuple(c['shape'])}")
+def test_oracle_e2h_and_poynting_match_reference(c):
+    H = O.e2h(complex(c['omega']), c['dxes'], c['x'], _opt(c, 'mu'), _opt(c, 'pmc'))
+    assert numpy.linalg.norm(H - c['H']) <= 1e-14 * numpy.linalg.norm(c['H'])
+    S = O.poynting_e_cross_h(c['dxes'], c['x'], c['H'].conj())
+    # the operator and the functional forms of the reference agree with each other
+    for ref in (c['S_op'], c['S_fn']):
+        assert numpy.linalg.norm(S - ref) <= 1e-14 * numpy.linalg.norm(ref)
 
 
 @pytest.mark.parametrize('c', OPS, ids=lambda c: f"op{c['index']}")
