@@ -404,6 +404,20 @@ def kernel_mode(args) -> None:
             (extra_c128 if prec == 'c128' else extra_c64)
         print(f'apply  A0_{prec:4s}               10 launches  {ms * 1e3:8.1f} us  '
               f'{per_cell * p.n_cells / (ms / 1e3) / 1e9:7.1f} GB/s algorithmic')
+    # E -> (H, E x conj(H)) in one pass: read E, write H and S (3 x 48 B per cell; mu and the
+    # mask byte when present)
+    for _ in range(3):
+        op.poynting(x)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(10):
+        op.poynting(x)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / 10
+    per_cell = 3 * 48 + (24 if p.mu is not None else 0) + (1 if p.pmc is not None else 0)
+    print(f'fields e2h+poynting c128         10 launches  {ms * 1e3:8.1f} us  '
+          f'{per_cell * p.n_cells / (ms / 1e3) / 1e9:7.1f} GB/s algorithmic')
 
 
 def gradient_check(args) -> dict:

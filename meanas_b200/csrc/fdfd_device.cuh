@@ -13,10 +13,10 @@
 //
 // Kernel shape: a CTA owns a TY x TZ tile of (y, z) columns and marches along x over
 // a chunk of planes.  Each step stages one x-plane of the input field (tile plus a
-// one-cell periodic halo in y and z) in shared memory; each thread forms H = ce(u) at
-// its own cell and at its j-1 and k-1 neighbours, then the curl of H.  H on plane i-1
-// (needed by dB_x) stays in registers, so every input value is read from memory once
-// per step (halo reads hit L1/L2) and a step needs one CTA barrier.  The input field is produced on the fly by a pointwise loader (for example
+// one-cell periodic halo in y and z) in shared memory, computes H = ce(u) on the tile
+// plus its low y/z halo, then the curl of H.  H on plane i-1 (needed by dB_x) stays in
+// registers, so every input value is read from memory once per step (halo reads hit
+// L1/L2).  The input field is produced on the fly by a pointwise loader (for example
 // r + beta * p in a Krylov step) and every own cell is handed, with its operator
 // value, to an epilogue that writes outputs and accumulates reductions; so the
 // Krylov vector updates and dot products ride on the same pass over HBM.
@@ -280,12 +280,11 @@ __device__ __forceinline__ void run_finish(const Op& o, const double* sums) {
 //            const cx<R> W[3], const R aW[3], const Pre& p, A* acc);   y = A0 u
 //   void finish(const double* sums) const;    last CTA, thread 0
 //
-// Pipeline per x plane i (U is a ring of three planes holding u on planes i and i+1;
-// Sbox/Sown receive the raw inputs of plane i+2):  wait for plane i+1's copies ->
-// convert them into U (u = make_u, PEC mask; own cells: convert_own) -> barrier ->
-// issue cp.async for plane i+2 -> H = ce(u) at the own cell and its j-1 / k-1
-// neighbours -> curl of H, epilogue.  Global loads of the box are asynchronous copies,
-// so they overlap the arithmetic of the previous plane.
+// Pipeline per x plane i (U holds u on planes i and i+1, Sbox/Sown the raw inputs of
+// plane i+2 in flight):  wait for plane i+1's copies -> convert them into U (u = make_u,
+// PEC mask; own cells: convert_own) -> issue cp.async for plane i+2 -> H = ce(u) on the
+// tile + low halo -> curl of H, epilogue.  Global loads of the box are asynchronous
+// copies, so they overlap the arithmetic of the previous plane.
 __device__ __forceinline__ void cp_async16(void* s, const void* g) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(g));
@@ -314,11 +313,13 @@ struct StencilShape {
   static constexpr int BH = TY + 2;            // box height (y)
   static constexpr int BOX = BW * BH;
   static constexpr int NHALO = BOX - NT;       // halo cells (<= NT)
-  static constexpr int NU = 3;                 // planes in the U ring
-  // shared memory: Sbox[NB][3][BOX] | Sown[NO][3][NT] | U[NU][3][BOX] | Xt | red[64]
+  static constexpr int HW = TZ + KZ;           // H plane width (own + low z halo)
+  static constexpr int HH = TY + 1;
+  // shared memory: Sbox[NB][3][BOX] | Sown[NO][3][NT] | U[2][3][BOX] | Hs[3][HH*HW] | Xt | red[64]
   static constexpr size_t off_own = sizeof(cx<R>) * (size_t)NB * 3 * BOX;
   static constexpr size_t off_u = off_own + sizeof(cx<R>) * (size_t)NO * 3 * NT;
-  static constexpr size_t off_xt = off_u + sizeof(cx<R>) * (size_t)NU * 3 * BOX;
+  static constexpr size_t off_h = off_u + sizeof(cx<R>) * (size_t)2 * 3 * BOX;
+  static constexpr size_t off_xt = off_h + sizeof(cx<R>) * (size_t)3 * HH * HW;
   static constexpr int XT_STRIDE = 6;  // per plane: idxe, idxh, dxe, dxh, (|dxe|, |dxh|)
   static constexpr size_t off_red = off_xt + sizeof(cx<R>) * (size_t)XT_STRIDE * (XC_MAX + 1);
   static constexpr size_t smem_bytes() { return off_red + 64 * sizeof(double); }
@@ -328,12 +329,13 @@ struct StencilShape {
 template <typename R, int TZ, int TY, bool FLAT, int MINB, class Op>
 __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op, RedBuf rb) {
   using S = StencilShape<R, TZ, TY, FLAT, Op::NB, Op::NO>;
-  constexpr int NT = S::NT, BW = S::BW, BOX = S::BOX, KZ = S::KZ;
+  constexpr int NT = S::NT, BW = S::BW, BOX = S::BOX, KZ = S::KZ, HW = S::HW, HH = S::HH;
   constexpr int NB = Op::NB, NO = Op::NO;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* Sbox = reinterpret_cast<cx<R>*>(smem_raw);                 // [NB][3][BOX]
   cx<R>* Sown = reinterpret_cast<cx<R>*>(smem_raw + S::off_own);    // [NO][3][NT]
-  cx<R>* U = reinterpret_cast<cx<R>*>(smem_raw + S::off_u);         // [NU][3][BOX]
+  cx<R>* U = reinterpret_cast<cx<R>*>(smem_raw + S::off_u);         // [2][3][BOX]
+  cx<R>* Hs = reinterpret_cast<cx<R>*>(smem_raw + S::off_h);        // [3][HH*HW]
   cx<R>* Xt = reinterpret_cast<cx<R>*>(smem_raw + S::off_xt);       // [XC+1][6]
   double* shred = reinterpret_cast<double*>(smem_raw + S::off_red);
 
@@ -380,15 +382,20 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
     off1 = wrapi(j0 - 1 + bj, g.Y) * g.Z + (FLAT ? 0 : wrapi(k0 - KZ + bk, g.Z));
   }
 
-  // per-thread y/z difference factors, and the forward factors of the two neighbours
-  // whose H the backward curl needs: row j-1 and column k-1
+  // per-thread y/z difference factors
   const cx<R> idye = g.idxe[1][jc], idyh = g.idxh[1][jc];
   const cx<R> idze = FLAT ? czero<R>() : g.idxe[2][kc];
   const cx<R> idzh = FLAT ? czero<R>() : g.idxh[2][kc];
-  const int jmc = wrapi(jc - 1, g.Y);
-  const int kmc = FLAT ? 0 : wrapi(kc - 1, g.Z);
-  const cx<R> idye_jm = g.idxe[1][jmc];
-  const cx<R> idze_km = FLAT ? czero<R>() : g.idxe[2][kmc];
+  const int jm = wrapi(j0 - 1, g.Y);
+  const int km = FLAT ? 0 : wrapi(k0 - 1, g.Z);
+  const int kh = FLAT ? 0 : kc;
+  // the low-y halo row (j0-1) is computed by warp-row ty == 0, the low-z halo column
+  // (k0-1) by lanes tz < TY of the last warp-row (lane tz handles row j0 + tz)
+  const bool row_halo = (ty == 0);
+  const bool col_halo = !FLAT && (ty == TY - 1) && (tz < TY);
+  const int jr = wrapi(j0 + (col_halo ? tz : 0), g.Y);
+  const cx<R> idy_halo = row_halo ? g.idxe[1][jm] : (col_halo ? g.idxe[1][jr] : czero<R>());
+  const cx<R> idze_km = FLAT ? czero<R>() : g.idxe[2][km];
 
   // per-plane x factors of this CTA's planes (plane x0-1 first) into shared memory
   for (int t = tid; t <= x1 - x0; t += NT) {
@@ -508,9 +515,9 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
     }
   };
 
-  // ---- prologue: planes x0-1 and x0 into U slots 0 and 1, H on plane x0-1 (own cell)
+  // ---- prologue: planes x0-1 and x0 into U, H on plane x0-1 (own cells: Hy, Hz)
   const int ip = wrapi(x0 - 1, g.X);
-  // (own slots only until the barrier: the barrier publishes Xt and both U planes)
+  // (own slots only until the barrier: the barrier publishes Xt, U[0] and U[1])
   issue(ip);
   cp_async_wait_all();
   convert(0, ip, false);
@@ -528,13 +535,13 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
     hy_prev = hy;
     hz_prev = hz;
   }
-  // One barrier per plane.  U is a ring of three planes: step i converts plane i+1 into
-  // the slot of plane i-2, whose last readers (step i-2) all finished before step i-1's
-  // barrier.  Each thread forms the H values of its j-1 and k-1 neighbours itself from U,
-  // so no H plane is shared between threads.
+  // The first step converts plane x0+1 into U[0]: every thread must be done reading
+  // U[0] (plane x0-1) for the prologue H.  (Inside the loop the previous step's Hs
+  // barrier gives this ordering.)
+  __syncthreads();
   int cur = 1;
   for (int i = x0; i < x1; ++i) {
-    const int nx = cur == S::NU - 1 ? 0 : cur + 1;
+    const int nxt = cur ^ 1;
     const int in1 = (i + 1 == g.X) ? 0 : i + 1;
     const int ibase = (int)i * YZ;
     const int cell = ibase + (int)jc * g.Z + kc;
@@ -546,37 +553,52 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
 #pragma unroll
       for (int c = 0; c < 3; ++c) e3[c] = g.eps[c * N + cell];
     }
-    // plane i+1's raw inputs landed (each thread copies and converts its own slots only)
+    // Plane i+1's raw inputs landed.  No barrier is needed here: every thread copies and
+    // converts only its own Sbox/Sown slots, U[nxt] (plane i-1) was last read before the
+    // previous step's Hs barrier, and Hs is rewritten only after the barrier below.
     cp_async_wait_all();
-    convert(nx, in1, i + 1 < x1);
-    __syncthreads();       // U[nx] = u(i+1) ready for the neighbours' differences
+    convert(nxt, in1, i + 1 < x1);
+    __syncthreads();       // U[nxt] = u(i+1) ready for the neighbours' differences
     if (i + 1 < x1) issue(in1 + 1 == g.X ? 0 : in1 + 1);
     const cx<R>* xe = Xt + (i - x0 + 1) * S::XT_STRIDE;
     const cx<R> idxe_i = xe[0], idxh_i = xe[1];
     cx<R> hx, hy, hz;
-    curl_e(cur, nx, ty + 1, tz + KZ, idye, idze, idxe_i, hx, hy, hz);
+    curl_e(cur, nxt, ty + 1, tz + KZ, idye, idze, idxe_i, hx, hy, hz);
     hscale(cell, hx, hy, hz);
-    cx<R> hx_jm, hz_jm;  // H at (j-1, k): Hx and Hz
-    {
-      cx<R> ay;
-      curl_e(cur, nx, ty, tz + KZ, idye_jm, idze, idxe_i, hx_jm, ay, hz_jm);
-      hscale(ibase + jmc * g.Z + kc, hx_jm, ay, hz_jm);
+    const int hp = (ty + 1) * HW + tz + KZ;
+    Hs[0 * HH * HW + hp] = hx;
+    Hs[1 * HH * HW + hp] = hy;
+    Hs[2 * HH * HW + hp] = hz;
+    if (row_halo) {  // low y halo row (j0-1)
+      cx<R> ax, ay, az;
+      curl_e(cur, nxt, 0, tz + KZ, idy_halo, idze, idxe_i, ax, ay, az);
+      hscale(ibase + (int)jm * g.Z + kh, ax, ay, az);
+      Hs[0 * HH * HW + tz + KZ] = ax;
+      Hs[1 * HH * HW + tz + KZ] = ay;
+      Hs[2 * HH * HW + tz + KZ] = az;
+    }
+    if (col_halo) {  // low z halo column (k0-1), row j0 + tz
+      cx<R> ax, ay, az;
+      curl_e(cur, nxt, tz + 1, 0, idy_halo, idze_km, idxe_i, ax, ay, az);
+      hscale(ibase + (int)jr * g.Z + km, ax, ay, az);
+      Hs[0 * HH * HW + (tz + 1) * HW] = ax;
+      Hs[1 * HH * HW + (tz + 1) * HW] = ay;
+      Hs[2 * HH * HW + (tz + 1) * HW] = az;
     }
     cx<R> u[3];
     u[0] = U[(cur * 3 + 0) * BOX + pos0];
     u[1] = U[(cur * 3 + 1) * BOX + pos0];
     u[2] = U[(cur * 3 + 2) * BOX + pos0];
+    __syncthreads();
+    const cx<R> hz_jm = Hs[2 * HH * HW + ty * HW + tz + KZ];
+    const cx<R> hx_jm = Hs[0 * HH * HW + ty * HW + tz + KZ];
     cx<R> y[3];
     if (FLAT) {
       y[0] = (hz - hz_jm) * idyh;
       y[1] = czero<R>() - (hz - hz_prev) * idxh_i;
     } else {
-      cx<R> hx_km, hy_km;  // H at (j, k-1): Hx and Hy
-      {
-        cx<R> bz;
-        curl_e(cur, nx, ty + 1, tz, idye, idze_km, idxe_i, hx_km, hy_km, bz);
-        hscale(ibase + (int)jc * g.Z + kmc, hx_km, hy_km, bz);
-      }
+      const cx<R> hy_km = Hs[1 * HH * HW + (ty + 1) * HW + tz];
+      const cx<R> hx_km = Hs[0 * HH * HW + (ty + 1) * HW + tz];
       y[0] = (hz - hz_jm) * idyh - (hy - hy_km) * idzh;
       y[1] = (hx - hx_km) * idzh - (hz - hz_prev) * idxh_i;
     }
@@ -596,7 +618,7 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
       if (Op::NEEDS_W) wyz.at(xe[2], xe[3], xe[4].re, xe[4].im, W, aW);
       o.own(cell, i, j, k, u, y, W, aW, pr, acc);
     }
-    cur = nx;
+    cur = nxt;
   }
   cp_async_wait_all();
 
