@@ -187,6 +187,19 @@ int fdfd_eps_gradient(fdfd_plan* plan, const void* E, const void* E_adj, double*
  * arrays; H may be NULL when only S is wanted. */
 int fdfd_e2h(fdfd_plan* plan, const void* E, void* H, void* S, int32_t flags, void* stream);
 
+/* fdfd_tfsf_source flags */
+#define FDFD_SRC_EDGES 1    /* e_boundary_source: keep J only where shifting Q changes it */
+#define FDFD_SRC_PERIODIC 2 /* with FDFD_SRC_EDGES: periodic_mask_edges = True */
+
+/* The step before the solve: J = e_tfsf_source(Q, omega, dxes, epsilon, mu) @ E
+ * (meanas/fdfd/operators.py:366-393: (A0 Q - Q A0) E / (-i omega), A0 = e_full without
+ * masks, Q = diag(tf_region)), or with FDFD_SRC_EDGES
+ * e_boundary_source(Q, ..., periodic_mask_edges) @ E (:396-450).  The plan must have no
+ * PEC/PMC (the reference's source operators take none).  E, J: complex128 [3N] device
+ * arrays (J must not alias E); tf_region: float64 [3N]. */
+int fdfd_tfsf_source(fdfd_plan* plan, const void* E, const double* tf_region, void* J, int32_t flags,
+                     void* stream);
+
 /* fdfd_residual without a workspace, for callers that cannot allocate device memory
  * (an exhausted or frozen allocator, or a host program that owns every device buffer
  * and can pass only inputs and outputs).  No counterpart in the reference.

@@ -92,7 +92,12 @@ EXPORTS = {
     'fdfd_eps_gradient': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     'fdfd_residual_static': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_void_p]),
     'fdfd_e2h': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    'fdfd_tfsf_source': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
 }
+
+# fdfd_tfsf_source flags
+SRC_EDGES = 1
+SRC_PERIODIC = 2
 
 # fdfd_e2h flags (include/meanas_fdfd.h)
 E2H_CONJ = 1

@@ -1071,6 +1071,26 @@ extern "C" int fdfd_e2h(fdfd_plan* P, const void* E, void* H, void* S, int32_t f
   return 0;
 }
 
+// ------------------------------------------------------------------ TFSF / boundary sources
+extern "C" int fdfd_tfsf_source(fdfd_plan* P, const void* E, const double* tf_region, void* J, int32_t flags,
+                                void* stream) {
+  if (!P || !E || !tf_region || !J) return set_err(FDFD_ERR_ARG, "fdfd_tfsf_source: NULL argument");
+  if (E == J) return set_err(FDFD_ERR_ARG, "fdfd_tfsf_source: J must not alias E");
+  if (flags & ~(FDFD_SRC_EDGES | FDFD_SRC_PERIODIC))
+    return set_err(FDFD_ERR_ARG, "fdfd_tfsf_source: unknown flags %d", flags);
+  if (P->has_mask)
+    return set_err(FDFD_ERR_ARG, "fdfd_tfsf_source: the source operator has no PEC/PMC; use a plan without masks");
+  const double m2 = P->om_re * P->om_re + P->om_im * P->om_im;
+  if (!(m2 > 0.0)) return set_err(FDFD_ERR_ARG, "fdfd_tfsf_source: omega is zero");
+  cudaStream_t s = (cudaStream_t)stream;
+  P->launches = 0;
+  OpTfsf<double> op{(const cx<double>*)E, tf_region, (cx<double>*)J, 0, (flags & FDFD_SRC_EDGES) != 0,
+                    (flags & FDFD_SRC_PERIODIC) != 0, mkc<double>(P->om_im / m2, P->om_re / m2), P->g64};
+  TRY(launch_stencil<double>(P, P->g64, 0, op, RedBuf{nullptr, nullptr}, s));
+  op.pass = 1;
+  return launch_stencil<double>(P, P->g64, 0, op, RedBuf{nullptr, nullptr}, s);
+}
+
 // ------------------------------------------------------------------ allocation-free residual
 // For callers that cannot allocate device memory at all (for example code running
 // under an allocator that is already exhausted or frozen, or a host application

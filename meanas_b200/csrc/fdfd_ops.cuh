@@ -954,6 +954,78 @@ struct OpCopy {
   __device__ void finish(const double*) const {}
 };
 
+// ------------------------------------------------------------------ TFSF / boundary sources
+// The step before the solve (meanas/fdfd/operators.py:366-450): the current that injects
+// a desired field E inside a total-field region Q,
+//   J = (A0 Q E - Q A0 E) / (-i omega),   A0 = e_full(omega, dxes, epsilon, mu) (no masks),
+// and, with `edges`, only on the cells where shifting Q by one cell along a non-singleton
+// axis changes it (e_boundary_source; `periodic` wraps the shift, otherwise the cell past
+// an edge mirrors back onto the edge cell, fdmath/operators.py:55-98).  Two stencil
+// passes, no scratch: pass 0 writes out = A0 (Q E); pass 1 reads it back and writes
+// out = jmask (out - Q A0 E) / (-i omega).
+template <typename R>
+struct OpTfsf {
+  static constexpr int NB = 1, NO = 0, NRED = 0;
+  static constexpr bool NEEDS_W = false;
+  const cx<R>* e;
+  const R* q;  // Q, per component (3N)
+  cx<R>* out;
+  int pass, edges, periodic;
+  cx<R> inv_miw;  // 1 / (-i omega)
+  Geo<R> g;
+  struct Pre {
+    cx<R> o[3];
+    R qv[3];
+  };
+  __device__ bool skip() const { return false; }
+  __device__ void prepare() {}
+  __device__ const cx<R>* box_src(int) const { return e; }
+  __device__ void pre(int cell, Pre& p) const {
+    if (pass == 0) return;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      p.o[c] = out[c * g.N + cell];
+      p.qv[c] = q[c * g.N + cell];
+    }
+  }
+  __device__ cx<R> make_u(const cx<R>* v, int idx, int) const { return pass == 0 ? q[idx] * v[0] : v[0]; }
+  __device__ const cx<R>* own_src(int) const { return nullptr; }
+  __device__ void convert_own(const cx<R>*, const cx<R>*, int, int, cx<R>, acc_t<R>*) const {}
+  // the index one cell away along `axis` (s = +-1): wrapped, or mirrored onto the edge cell
+  __device__ int step(int v, int n, int s) const {
+    v += s;
+    if (periodic) return v < 0 ? n - 1 : (v >= n ? 0 : v);
+    return v < 0 ? 0 : (v >= n ? n - 1 : v);
+  }
+  __device__ bool on_edge(int c, int i, int j, int k) const {
+    const int YZ = g.Y * g.Z, base = c * g.N;
+    const R q0 = q[base + i * YZ + j * g.Z + k];
+    bool m = false;
+#pragma unroll
+    for (int s = -1; s <= 1; s += 2) {
+      if (g.X > 1) m |= q[base + step(i, g.X, s) * YZ + j * g.Z + k] != q0;
+      if (g.Y > 1) m |= q[base + i * YZ + step(j, g.Y, s) * g.Z + k] != q0;
+      if (g.Z > 1) m |= q[base + i * YZ + j * g.Z + step(k, g.Z, s)] != q0;
+    }
+    return m;
+  }
+  __device__ void own(int cell, int i, int j, int k, const cx<R>*, const cx<R> yv[3], const cx<R>*, const R*,
+                      const Pre& p, acc_t<R>*) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int idx = c * g.N + cell;
+      if (pass == 0) {
+        out[idx] = yv[c];
+      } else {
+        cx<R> v = (p.o[c] - p.qv[c] * yv[c]) * inv_miw;
+        if (edges && !on_edge(c, i, j, k)) v = czero<R>();
+        out[idx] = v;
+      }
+    }
+  }
+  __device__ void finish(const double*) const {}
+};
+
 // ------------------------------------------------------------------ E -> H, E x H
 // The step after the solve: H = pm mu^-1 ce(E) / (-i omega) (the sparse e2h of
 // meanas/fdfd/operators.py:253-282) and, when S is set, S = E x H' with H' = conj(H)

@@ -1,6 +1,14 @@
-"""The step after the solve on the GPU: E -> H and the Poynting cross product.
+"""The steps either side of the solve on the GPU: sources, E -> H, Poynting products.
 
-Drop-ins for the reference's post-processing of a ``generic()`` result:
+Drop-ins for the reference's source construction (before ``generic()``):
+
+* ``e_tfsf_source(TF_region, omega, dxes, epsilon, mu=None)``
+  ``meanas/fdfd/operators.py:366-393``: ``op @ E`` is the current that injects E inside
+  the total-field region.
+* ``e_boundary_source(mask, omega, dxes, epsilon, mu=None, periodic_mask_edges=False)``
+  ``meanas/fdfd/operators.py:396-450``: the same, kept on the edges of the mask.
+
+and for the post-processing of a ``generic()`` result:
 
 * ``e2h(omega, dxes, mu=None, pmc=None)``        ``meanas/fdfd/operators.py:253-282``
   (a sparse matrix there; here a matrix-free operator used the same way, ``op @ E``).
@@ -72,3 +80,23 @@ def poynting_e_cross_h(dxes, *, device: Any | None = None) -> Callable[[Any, Any
         S, _ = grid.poynting(as_device(e, torch.complex128, grid.device, grid.n, 'e'), h, conj=False)
         return _out(e, S.reshape(shape))
     return exh
+
+
+def e_tfsf_source(TF_region, omega: complex, dxes, epsilon, mu=None, *,
+                  device: Any | None = None) -> FieldOperator:
+    """``(A0 Q - Q A0) / (-i omega)`` with ``Q = diag(TF_region)`` as ``op @ E``
+    (``meanas/fdfd/operators.py:366-393``; ``A0`` without PEC/PMC, as there)."""
+    grid = GridOperator(omega, dxes, epsilon, mu, device=device, fp32=False)
+    q = as_device(TF_region, torch.float64, grid.device, grid.n, 'TF_region')
+    return FieldOperator(lambda e: _out(e, grid.tfsf_source(e, q)), grid.n)
+
+
+def e_boundary_source(mask, omega: complex, dxes, epsilon, mu=None, periodic_mask_edges: bool = False, *,
+                      device: Any | None = None) -> FieldOperator:
+    """``e_tfsf_source`` kept only where shifting ``mask`` by one cell along a non-singleton
+    axis changes it (``meanas/fdfd/operators.py:396-450``; past the grid edge the shift
+    mirrors, or wraps with ``periodic_mask_edges``)."""
+    grid = GridOperator(omega, dxes, epsilon, mu, device=device, fp32=False)
+    q = as_device(mask, torch.float64, grid.device, grid.n, 'mask')
+    return FieldOperator(lambda e: _out(e, grid.tfsf_source(e, q, edges=True, periodic=periodic_mask_edges)),
+                         grid.n)

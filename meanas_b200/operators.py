@@ -249,6 +249,21 @@ class GridOperator:
                                          _stream_handle()))
         return S, Ht
 
+    def tfsf_source(self, E, tf_region, *, edges: bool = False, periodic: bool = False,
+                    out: torch.Tensor | None = None) -> torch.Tensor:
+        """``J = (A0 Q - Q A0) E / (-i omega)`` with ``Q = diag(tf_region)``
+        (``meanas/fdfd/operators.py:366-393``); ``edges`` keeps J only where shifting Q by one
+        cell changes it (``e_boundary_source``, ``:396-450``; ``periodic`` =
+        ``periodic_mask_edges``).  The operator must have no PEC/PMC."""
+        Et = as_device(E, torch.complex128, self.device, self.n, 'E')
+        q = as_device(tf_region, torch.float64, self.device, self.n, 'tf_region')
+        J = out if out is not None else torch.empty_like(Et)
+        flags = (_lib.SRC_EDGES if edges else 0) | (_lib.SRC_PERIODIC if periodic else 0)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.fdfd_tfsf_source(self.plan, Et.data_ptr(), q.data_ptr(), J.data_ptr(), flags,
+                                                 _stream_handle()))
+        return J
+
     # ------------------------------------------------------------------ solve
     def solve_opts(self, *, method: str = 'cocg', rtol: float = 1e-8, atol: float = 0.0,
                    maxiter: int | None = None, criterion: str = 'true', adjoint: bool = False,

@@ -33,6 +33,10 @@ What each function restates:
 * ``poynting_e_cross_h``  ``E x H`` with the one-cell shift of E and the cell-width
   weights of ``meanas/fdfd/functional.py:187-221`` (the same product as
   ``operators.poynting_e_cross(E) @ H``, ``meanas/fdfd/operators.py:310-336``).
+* ``tfsf_source``    ``(A0 Q - Q A0) E / (-i omega)`` with ``A0`` unmasked
+  (``meanas/fdfd/operators.py:366-393``) and, with ``edges``, the edge mask of
+  ``e_boundary_source`` (``:396-450``; mirrored or periodic one-cell shifts,
+  ``meanas/fdmath/operators.py:55-98``).
 * ``cocg``           complex-symmetric CG in the E-space with the ``p^2``-weighted
   bilinear form: algebraically the COCG iteration on ``Pl A0 Pr`` (the system
   ``generic()`` builds) rewritten with ``x = Pl E``; the GPU solver runs the same
@@ -129,6 +133,31 @@ def poynting_e_cross_h(dxes, E, H) -> NDArray:
     s[1] = numpy.roll(ez, -1, axis=1) * hx - numpy.roll(ex, -1, axis=1) * hz
     s[2] = numpy.roll(ex, -1, axis=2) * hy - numpy.roll(ey, -1, axis=2) * hx
     return s.ravel()
+
+
+def _edge_mask(q: NDArray, periodic: bool) -> NDArray:
+    """Cells of a (3,X,Y,Z) array where a one-cell shift along a non-singleton axis changes it."""
+    m = numpy.zeros(q.shape, dtype=bool)
+    for axis in (1, 2, 3):
+        n = q.shape[axis]
+        if n == 1:
+            continue
+        for s in (-1, 1):
+            idx = numpy.arange(n) + s
+            idx = idx % n if periodic else numpy.clip(idx, 0, n - 1)
+            m |= numpy.take(q, idx, axis=axis) != q
+    return m
+
+
+def tfsf_source(omega, dxes, epsilon, E, tf_region, mu=None, *, edges=False, periodic=False) -> NDArray:
+    """``J = (A0 Q E - Q A0 E) / (-i omega)``, optionally on the edges of Q only; (3XYZ,)."""
+    q = numpy.asarray(tf_region, dtype=float)
+    e = numpy.asarray(E, dtype=complex)
+    j = (e_full_apply(omega, dxes, epsilon, q * e, mu) - q * e_full_apply(omega, dxes, epsilon, e, mu)) / (-1j * omega)
+    if edges:
+        shape = _shape_of(dxes)
+        j = j * _edge_mask(q.reshape(3, *shape), periodic).ravel()
+    return j
 
 
 def precond_p2(dxes) -> NDArray:

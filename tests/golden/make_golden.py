@@ -20,6 +20,9 @@ the only place that reads it.  Outputs:
                     ``operators.poynting_e_cross(x) @ conj(H)`` and
                     ``functional.poynting_e_cross_h(dxes)(x, conj(H))`` on random
                     small problems.
+* ``sources.npz``   ``operators.e_tfsf_source(Q, ...) @ x`` and
+                    ``operators.e_boundary_source(Q, ..., periodic_mask_edges) @ x`` for
+                    box-shaped and random total-field regions.
 * ``dipole48.npz``  reference ``generic()`` on the 48^3 dipole-in-core problem
                     (rtol 1e-8, scipy QMR): field stored as complex64.
 """
@@ -162,6 +165,51 @@ def gen_e2h() -> None:
     numpy.savez_compressed(OUT / 'e2h.npz', **out)
 
 
+def gen_sources() -> None:
+    rng = numpy.random.default_rng(5)
+    out = {}
+    cases = [((10, 9, 8), True, 'box', 2),
+             ((12, 7, 1), False, 'box', 2),
+             ((1, 9, 11), True, 'random', 0),
+             ((8, 8, 8), False, 'random', 3),
+             ((16, 11, 13), True, 'box', 3)]
+    for n, (shape, use_mu, kind, th) in enumerate(cases):
+        om = complex(2 * numpy.pi / rng.uniform(6, 12), 0.0)
+        dxes = [[rng.uniform(0.8, 1.3, s) for s in shape] for _ in range(2)]
+        sf = scpml.prepare_s_function(ln_R=-16, m=3.5)
+        for ax in range(3):
+            if shape[ax] > 2 * th + 1 and th > 0:
+                for pol in (-1, 1):
+                    dxes = scpml.stretch_with_scpml(dxes, axis=ax, polarity=pol, omega=om.real,
+                                                    thickness=th, s_function=sf)
+        N3 = 3 * int(numpy.prod(shape))
+        eps = rng.uniform(1, 12.1, N3)
+        mu = rng.uniform(1, 1.5, N3) if use_mu else None
+        if kind == 'box':
+            q = numpy.zeros((3, *shape))
+            sl = tuple(slice(s // 4, max(s // 4 + 1, 3 * s // 4)) for s in shape)
+            q[(slice(None), *sl)] = 1.0
+            q = q.ravel()
+        else:
+            q = (rng.random(N3) < 0.3).astype(float)
+        x = rng.standard_normal(N3) + 1j * rng.standard_normal(N3)
+        p = f'c{n}_'
+        out[p + 'shape'] = numpy.array(shape)
+        out[p + 'omega'] = numpy.array(om)
+        pack_dxes(p, dxes, out)
+        out[p + 'eps'] = eps
+        if mu is not None:
+            out[p + 'mu'] = mu
+        out[p + 'q'] = q
+        out[p + 'x'] = x
+        out[p + 'tfsf'] = operators.e_tfsf_source(q, om, dxes, eps, mu) @ x
+        out[p + 'edge_mirror'] = operators.e_boundary_source(q, om, dxes, eps, mu) @ x
+        out[p + 'edge_periodic'] = operators.e_boundary_source(q, om, dxes, eps, mu,
+                                                               periodic_mask_edges=True) @ x
+    out['n'] = numpy.array(len(cases))
+    numpy.savez_compressed(OUT / 'sources.npz', **out)
+
+
 def gen_solve() -> None:
     """Reference generic() solutions."""
     rng = numpy.random.RandomState(12345)
@@ -300,7 +348,7 @@ def gen_dipole48() -> None:
 
 
 if __name__ == '__main__':
-    which = sys.argv[2:] or ['scpml', 'operator', 'e2h', 'solve', 'dipole48']
+    which = sys.argv[2:] or ['scpml', 'operator', 'e2h', 'sources', 'solve', 'dipole48']
     for w in which:
         t = time.perf_counter()
         globals()[f'gen_{w}']()

@@ -80,3 +80,29 @@ def test_poynting_planes_like_reference_test(cuda, c):
     dv = (c['dxes'][0][0][:, None, None] * c['dxes'][0][1][None, :, None] * c['dxes'][0][2][None, None, :])
     src_energy = -((e * J.conj()).real * dv)[:, mask] / 2
     numpy.testing.assert_allclose(sum(planes), src_energy.sum(), rtol=1e-6)
+
+
+SOURCES = golden_cases('sources')
+
+
+@pytest.mark.parametrize('c', SOURCES, ids=lambda c: f"src{c['index']}-{tuple(int(s) for s in c['shape'])}")
+def test_tfsf_and_boundary_sources_match_reference(cuda, c):
+    from meanas_b200 import fields
+    om, mu = complex(c['omega']), c.get('mu')
+    args = (c['q'], om, c['dxes'], c['eps'], mu)
+    J = fields.e_tfsf_source(*args, device=cuda) @ c['x']
+    assert _rel(J, c['tfsf']) <= 1e-13
+    for periodic, key in ((False, 'edge_mirror'), (True, 'edge_periodic')):
+        Jb = fields.e_boundary_source(*args, periodic_mask_edges=periodic, device=cuda) @ c['x']
+        assert _rel(Jb, c[key]) <= 1e-13
+        # the edge mask is exact: the same cells are zero
+        assert numpy.array_equal(Jb == 0, c[key] == 0)
+
+
+def test_source_operator_refuses_masked_plans(cuda):
+    from meanas_b200 import _lib
+    from meanas_b200.operators import GridOperator
+    c = SOURCES[0]
+    grid = GridOperator(complex(c['omega']), c['dxes'], c['eps'], pec=numpy.zeros_like(c['eps']), device=cuda)
+    with pytest.raises(_lib.FDFDError, match='no PEC/PMC'):
+        grid.tfsf_source(c['x'], c['q'])

@@ -11,6 +11,7 @@ from meanas_b200 import scpml
 OPS = golden_cases('operator')
 SOLVES = golden_cases('solve')
 E2H = golden_cases('e2h')
+SOURCES = golden_cases('sources')
 
 
 def _opt(c, k):
@@ -33,6 +34,16 @@ def test_oracle_e2h_and_poynting_match_reference(c):
     # the operator and the functional forms of the reference agree with each other
     for ref in (c['S_op'], c['S_fn']):
         assert numpy.linalg.norm(S - ref) <= 1e-14 * numpy.linalg.norm(ref)
+
+
+@pytest.mark.parametrize('c', SOURCES, ids=lambda c: f"src{c['index']}-{tuple(c['shape'])}")
+def test_oracle_sources_match_reference(c):
+    args = (complex(c['omega']), c['dxes'], c['eps'], c['x'], c['q'], _opt(c, 'mu'))
+    for kw, key in ((dict(), 'tfsf'), (dict(edges=True), 'edge_mirror'),
+                    (dict(edges=True, periodic=True), 'edge_periodic')):
+        j = O.tfsf_source(*args, **kw)
+        assert numpy.linalg.norm(j - c[key]) <= 1e-14 * numpy.linalg.norm(c[key])
+        assert numpy.array_equal(j == 0, c[key] == 0)
 
 
 @pytest.mark.parametrize('c', OPS, ids=lambda c: f"op{c['index']}")
