@@ -220,8 +220,10 @@ def true_residual(omega, dxes, epsilon, E, J, mu=None, pec=None, pmc=None) -> fl
 
 
 def generic_qmr(omega, dxes, J, epsilon, mu=None, *, pec=None, pmc=None, adjoint=False,
-                rtol=1e-8, atol=0.0, maxiter=None, E_guess=None, counter=None):
-    """Reference ``generic()`` + ``_scipy_qmr`` on the CPU: assemble, symmetrise, scipy QMR."""
+                rtol=1e-8, atol=0.0, maxiter=None, E_guess=None, counter=None, matrix_solver=None):
+    """Reference ``generic()`` + ``_scipy_qmr`` on the CPU: assemble, symmetrise, scipy QMR.
+    ``matrix_solver(A, b, **opts) -> x`` replaces QMR as the reference's hook of that name
+    does (``meanas/fdfd/solvers.py:97-103,134``); it then returns ``(E, None)``."""
     b0 = -1j * omega * numpy.asarray(J)
     A0 = e_full_csr(omega, dxes, epsilon, mu, pec, pmc)
     pl = precond_pl(dxes)
@@ -242,7 +244,11 @@ def generic_qmr(omega, dxes, J, epsilon, mu=None, *, pec=None, pmc=None, adjoint
         def cb(_xk):
             counter[0] += 1
         kw['callback'] = cb
-    x, info = scipy.sparse.linalg.qmr(A.tocsr(), b, **kw)
+    if matrix_solver is not None:
+        kw.pop('callback', None)
+        x, info = matrix_solver(A.tocsr(), b, **kw), None
+    else:
+        x, info = scipy.sparse.linalg.qmr(A.tocsr(), b, **kw)
     E = (Pl.conj().T @ x) if adjoint else (Pr @ x)
     return E, info
 
