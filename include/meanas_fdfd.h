@@ -200,6 +200,31 @@ int fdfd_e2h(fdfd_plan* plan, const void* E, void* H, void* S, int32_t flags, vo
 int fdfd_tfsf_source(fdfd_plan* plan, const void* E, const double* tf_region, void* J, int32_t flags,
                      void* stream);
 
+/* A general complex128 CSR matrix (device arrays), as scipy.sparse.csr_array holds it:
+ * row r's nonzeros are data[indptr[r] .. indptr[r+1]) at columns indices[...]. */
+typedef struct fdfd_csr_desc {
+  int64_t n;              /* rows = columns (< 2^31)                    */
+  int64_t nnz;
+  const int64_t* indptr;  /* int64[n + 1]                               */
+  const int32_t* indices; /* int32[nnz]                                 */
+  const void* data;       /* complex128[nnz]                            */
+} fdfd_csr_desc;
+
+/* y = A x for a CSR matrix (x, y: complex128[n], distinct). */
+int fdfd_csr_spmv(const fdfd_csr_desc* A, const void* x, void* y, void* stream);
+
+/* Workspace bytes of fdfd_csr_solve (7 complex128[n] vectors + scalar state). */
+int fdfd_csr_solve_workspace_bytes(const fdfd_csr_desc* A, size_t* bytes);
+
+/* Solve A x = b for a general CSR matrix with complex128 BiCGSTAB: the reference's
+ * second plugin point, matrix_solver(A, b, **opts) -> x (meanas/fdfd/solvers.py:97-103,134,
+ * whose default _scipy_qmr is :21-63).  Stops when ||r|| <= max(rtol ||b||, atol) on the
+ * recurrence residual (scipy's rule) or after opts->maxiter iterations; uses rtol, atol,
+ * maxiter and has_guess (x holds x0 on entry) of `opts`.  info->residual is the true
+ * ||b - A x|| / ||b|| of the returned x, which is the last iterate whatever the status. */
+int fdfd_csr_solve(const fdfd_csr_desc* A, const fdfd_solve_opts* opts, const void* b, void* x, void* ws,
+                   size_t ws_bytes, fdfd_solve_info* info, void* stream);
+
 /* fdfd_residual without a workspace, for callers that cannot allocate device memory
  * (an exhausted or frozen allocator, or a host program that owns every device buffer
  * and can pass only inputs and outputs).  No counterpart in the reference.

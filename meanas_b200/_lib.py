@@ -74,6 +74,11 @@ class SolveInfo(C.Structure):
     ]
 
 
+class CsrDesc(C.Structure):  # fdfd_csr_desc
+    _fields_ = [('n', C.c_int64), ('nnz', C.c_int64), ('indptr', C.c_void_p), ('indices', C.c_void_p),
+                ('data', C.c_void_p)]
+
+
 EXPORTS = {
     'fdfd_abi_version': (C.c_int, []),
     'fdfd_last_error': (C.c_char_p, []),
@@ -93,6 +98,10 @@ EXPORTS = {
     'fdfd_residual_static': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_void_p]),
     'fdfd_e2h': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     'fdfd_tfsf_source': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    'fdfd_csr_spmv': (C.c_int, [C.POINTER(CsrDesc), C.c_void_p, C.c_void_p, C.c_void_p]),
+    'fdfd_csr_solve_workspace_bytes': (C.c_int, [C.POINTER(CsrDesc), C.POINTER(C.c_size_t)]),
+    'fdfd_csr_solve': (C.c_int, [C.POINTER(CsrDesc), C.POINTER(SolveOpts), C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_size_t, C.POINTER(SolveInfo), C.c_void_p]),
 }
 
 # fdfd_tfsf_source flags

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../../include/meanas_fdfd.h"
+#include "fdfd_csr.cuh"
 #include "fdfd_ops.cuh"
 
 using namespace fdfd;
@@ -1089,6 +1090,137 @@ extern "C" int fdfd_tfsf_source(fdfd_plan* P, const void* E, const double* tf_re
   TRY(launch_stencil<double>(P, P->g64, 0, op, RedBuf{nullptr, nullptr}, s));
   op.pass = 1;
   return launch_stencil<double>(P, P->g64, 0, op, RedBuf{nullptr, nullptr}, s);
+}
+
+// ------------------------------------------------------------------ CSR solves
+static int csr_view(const fdfd_csr_desc* d, CsrView* v, const char* who) {
+  if (!d) return set_err(FDFD_ERR_ARG, "%s: NULL matrix", who);
+  if (d->n < 1 || d->n >= (int64_t)1 << 31) return set_err(FDFD_ERR_ARG, "%s: n = %lld out of range", who,
+                                                            (long long)d->n);
+  if (d->nnz < 0) return set_err(FDFD_ERR_ARG, "%s: nnz = %lld", who, (long long)d->nnz);
+  if (!d->indptr || (d->nnz > 0 && (!d->indices || !d->data)))
+    return set_err(FDFD_ERR_ARG, "%s: NULL CSR array", who);
+  v->n = (int)d->n;
+  v->indptr = (const long long*)d->indptr;
+  v->indices = (const int*)d->indices;
+  v->data = (const cx<double>*)d->data;
+  return 0;
+}
+
+// CTAs for the CSR kernels: enough rows per CTA step to cover n, at most 8 per SM
+static unsigned csr_blocks(int n) {
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const long long rows_per_cta = CSR_NT / CSR_LPR;
+  const long long need = (n + rows_per_cta - 1) / rows_per_cta;
+  return (unsigned)std::max(1LL, std::min(need, 8LL * nsm));
+}
+
+extern "C" int fdfd_csr_spmv(const fdfd_csr_desc* d, const void* x, void* y, void* stream) {
+  CsrView A;
+  TRY(csr_view(d, &A, "fdfd_csr_spmv"));
+  if (!x || !y) return set_err(FDFD_ERR_ARG, "fdfd_csr_spmv: NULL vector");
+  if (x == y) return set_err(FDFD_ERR_ARG, "fdfd_csr_spmv: y must not alias x");
+  k_csr_spmv<<<csr_blocks(A.n), CSR_NT, 0, (cudaStream_t)stream>>>(A, (const cx<double>*)x, (cx<double>*)y);
+  CKL();
+  return 0;
+}
+
+struct CsrLayout {
+  size_t state, ticket, partials, res, vec, total;
+};
+
+static CsrLayout csr_layout(int n) {
+  CsrLayout L;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off = align256(off + bytes);
+    return o;
+  };
+  L.state = take(sizeof(KState));
+  L.ticket = take(sizeof(unsigned));
+  L.partials = take(sizeof(double) * 8 * (size_t)8 * 2048);  // up to 8 sums x 16k CTAs
+  L.res = take(2 * sizeof(double));
+  L.vec = take(7 * 16 * (size_t)n);
+  L.total = off;
+  return L;
+}
+
+extern "C" int fdfd_csr_solve_workspace_bytes(const fdfd_csr_desc* d, size_t* bytes) {
+  CsrView A;
+  TRY(csr_view(d, &A, "fdfd_csr_solve_workspace_bytes"));
+  if (!bytes) return set_err(FDFD_ERR_ARG, "fdfd_csr_solve_workspace_bytes: NULL output");
+  *bytes = csr_layout(A.n).total;
+  return 0;
+}
+
+extern "C" int fdfd_csr_solve(const fdfd_csr_desc* d, const fdfd_solve_opts* o, const void* b, void* x, void* ws,
+                              size_t ws_bytes, fdfd_solve_info* info, void* stream) {
+  CsrView A;
+  TRY(csr_view(d, &A, "fdfd_csr_solve"));
+  if (!o || !b || !x || !ws) return set_err(FDFD_ERR_ARG, "fdfd_csr_solve: NULL argument");
+  const CsrLayout L = csr_layout(A.n);
+  if (ws_bytes < L.total) return set_err(FDFD_ERR_WORKSPACE, "fdfd_csr_solve: workspace %zu < %zu", ws_bytes,
+                                         L.total);
+  if (((uintptr_t)ws & 255) != 0) return set_err(FDFD_ERR_ARG, "fdfd_csr_solve: workspace not 256-byte aligned");
+  cudaStream_t s = (cudaStream_t)stream;
+  char* w = (char*)ws;
+  KState* st = (KState*)(w + L.state);
+  RedBuf rb{(double*)(w + L.partials), (unsigned*)(w + L.ticket)};
+  const size_t vb = 16 * (size_t)A.n;
+  cx<double>* V = (cx<double>*)(w + L.vec);
+  CsrBufs B{V, (cx<double>*)((char*)V + vb), (cx<double>*)((char*)V + 2 * vb), (cx<double>*)((char*)V + 3 * vb),
+            (cx<double>*)((char*)V + 4 * vb), (cx<double>*)((char*)V + 5 * vb), (cx<double>*)((char*)V + 6 * vb),
+            (cx<double>*)x, (const cx<double>*)b};
+  KState h{};
+  h.rtol = o->rtol;
+  h.atol = o->atol;
+  h.maxiter = o->maxiter > 0 ? o->maxiter : 10 * A.n;
+  h.status = ST_RUNNING;
+  CK(cudaMemcpyAsync(st, &h, sizeof(KState), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(rb.ticket, 0, sizeof(unsigned), s));
+  const unsigned grid = csr_blocks(A.n);
+  const unsigned seed = 0x5eed5eedU;
+  int launches = 0;
+  k_csr_init<<<grid, CSR_NT, 0, s>>>(A, B, o->has_guess != 0, seed, st, rb);
+  CKL();
+  ++launches;
+  const int chunk = o->chunk > 0 ? o->chunk : 16;
+  int status = ST_RUNNING, iters = 0;
+  for (;;) {
+    int head[4];  // crit, iter, maxiter, status
+    CK(cudaMemcpyAsync(head, &st->crit, sizeof(head), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    iters = head[1];
+    status = head[3];
+    if (status != ST_RUNNING || iters >= h.maxiter) break;
+    for (int it = 0; it < chunk; ++it) {
+      k_csr_a<<<grid, CSR_NT, 0, s>>>(A, B, seed, st, rb);
+      k_csr_b<<<grid, CSR_NT, 0, s>>>(A, B, st, rb);
+      k_csr_c<<<grid, CSR_NT, 0, s>>>(A, B, seed, st, rb);
+      CKL();
+      launches += 3;
+    }
+  }
+  if (status == ST_RUNNING) status = ST_MAXITER;
+  double* res = (double*)(w + L.res);
+  k_csr_residual<<<grid, CSR_NT, 0, s>>>(A, (const cx<double>*)x, (const cx<double>*)b, res, rb);
+  CKL();
+  ++launches;
+  double hr[2];
+  CK(cudaMemcpyAsync(hr, res, sizeof(hr), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (info) {
+    *info = fdfd_solve_info{};
+    info->status = status;
+    info->iterations = iters;
+    info->kernel_launches = launches;
+    info->residual = hr[1] > 0 ? std::sqrt(hr[0] / hr[1]) : std::sqrt(hr[0]);
+    info->residual_pc = info->residual;
+  }
+  return status == ST_CONVERGED ? 0 : status;
 }
 
 // ------------------------------------------------------------------ allocation-free residual

@@ -42,9 +42,9 @@ def test_struct_layouts_match_header(tmp_path: Path):
 #include <stddef.h>
 #include "{HEADER}"
 int main(void) {{
-  printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(fdfd_grid_desc), sizeof(fdfd_solve_opts),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(fdfd_grid_desc), sizeof(fdfd_solve_opts),
          sizeof(fdfd_solve_info), offsetof(fdfd_grid_desc, epsilon), offsetof(fdfd_solve_opts, history),
-         offsetof(fdfd_solve_info, residual));
+         offsetof(fdfd_solve_info, residual), sizeof(fdfd_csr_desc), offsetof(fdfd_csr_desc, data));
   return 0;
 }}
 ''')
@@ -52,7 +52,8 @@ int main(void) {{
     subprocess.run([cc, str(src), '-o', str(exe)], check=True)
     got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     want = [C.sizeof(_lib.GridDesc), C.sizeof(_lib.SolveOpts), C.sizeof(_lib.SolveInfo),
-            _lib.GridDesc.epsilon.offset, _lib.SolveOpts.history.offset, _lib.SolveInfo.residual.offset]
+            _lib.GridDesc.epsilon.offset, _lib.SolveOpts.history.offset, _lib.SolveInfo.residual.offset,
+            C.sizeof(_lib.CsrDesc), _lib.CsrDesc.data.offset]
     assert got == want
 
 
@@ -71,6 +72,18 @@ def test_argument_errors_need_no_gpu():
     assert lib.fdfd_plan_workspace_bytes(C.byref(d), C.byref(nbytes)) == 0
     assert nbytes.value > 3 * 120 * 8
     assert lib.fdfd_plan_destroy(None) == 0
+
+
+def test_csr_argument_checks_and_workspace_need_no_gpu():
+    from meanas_b200 import _lib
+    lib = _lib.load()
+    d = _lib.CsrDesc(0, 0, None, None, None)
+    nbytes = C.c_size_t()
+    assert lib.fdfd_csr_solve_workspace_bytes(C.byref(d), C.byref(nbytes)) == -1
+    assert b'n = 0' in lib.fdfd_last_error()
+    d = _lib.CsrDesc(1000, 13000, 1, 1, 1)  # any non-NULL pointers: only the layout is computed
+    assert lib.fdfd_csr_solve_workspace_bytes(C.byref(d), C.byref(nbytes)) == 0
+    assert nbytes.value >= 7 * 16 * 1000
 
 
 def test_no_cpu_fallback_in_product_package():
