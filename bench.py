@@ -418,6 +418,33 @@ def kernel_mode(args) -> None:
     per_cell = 3 * 48 + (24 if p.mu is not None else 0) + (1 if p.pmc is not None else 0)
     print(f'fields e2h+poynting c128         10 launches  {ms * 1e3:8.1f} us  '
           f'{per_cell * p.n_cells / (ms / 1e3) / 1e9:7.1f} GB/s algorithmic')
+    # CSR product of the matrix_solver hook on a matrix shaped like the assembled operator:
+    # 3N rows, 13 nonzeros per row at the curl-curl stencil's column offsets (synthetic
+    # values); bytes = values + column indices + row pointers + x once + y
+    from scipy import sparse
+    from meanas_b200.csr import CsrMatrix
+    X, Y, Z = p.shape
+    n = p.n_unknowns
+    N = p.n_cells
+    offs = numpy.array([0, 1, -1, Z, -Z, Y * Z, -Y * Z, N, -N, N + 1, N - Z, 2 * N, -2 * N + Y * Z])
+    rows = numpy.repeat(numpy.arange(n, dtype=numpy.int64), offs.size)
+    cols = (rows + numpy.tile(offs, n)) % n
+    rng = numpy.random.default_rng(0)
+    A = sparse.csr_array((rng.standard_normal(rows.size) + 1j, (rows, cols)), shape=(n, n))
+    M = CsrMatrix(A, dev)
+    del A, rows, cols
+    for _ in range(3):
+        M @ x
+    a.record()
+    for _ in range(10):
+        M @ x
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / 10
+    nnz = int(M.data.numel())
+    csr_bytes = nnz * (16 + 4) + (n + 1) * 8 + 2 * 16 * n
+    print(f'csr    spmv c128 ({nnz / n:.0f} nnz/row)   10 launches  {ms * 1e3:8.1f} us  '
+          f'{csr_bytes / (ms / 1e3) / 1e9:7.1f} GB/s algorithmic')
 
 
 def gradient_check(args) -> dict:
