@@ -421,6 +421,8 @@ def kernel_mode(args) -> None:
     # CSR product of the matrix_solver hook on a matrix shaped like the assembled operator:
     # 3N rows, 13 nonzeros per row at the curl-curl stencil's column offsets (synthetic
     # values); bytes = values + column indices + row pointers + x once + y
+    if p.n_unknowns > 12_000_000:
+        return
     from scipy import sparse
     from meanas_b200.csr import CsrMatrix
     X, Y, Z = p.shape
