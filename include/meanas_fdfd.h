@@ -225,6 +225,43 @@ int fdfd_csr_solve_workspace_bytes(const fdfd_csr_desc* A, size_t* bytes);
 int fdfd_csr_solve(const fdfd_csr_desc* A, const fdfd_solve_opts* opts, const void* b, void* x, void* ws,
                    size_t ws_bytes, fdfd_solve_info* info, void* stream);
 
+/* ---- FDTD (time domain) ----
+ * The Yee updates of meanas/fdtd: maxwell_h / maxwell_e (meanas/fdtd/base.py:13-125) and
+ * updates_with_cpml (meanas/fdtd/pml.py:115-230), on real fields of 3 x X x Y x Z
+ * (float32 or float64), with the arithmetic of the reference step by step, so results are
+ * the same bits. */
+#define FDFD_REAL64 0
+#define FDFD_REAL32 1
+#define FDFD_FDTD_PLAIN 0 /* maxwell_h / maxwell_e                   */
+#define FDFD_FDTD_CPML 1  /* updates_with_cpml (CPML on the faces set) */
+
+typedef struct fdfd_fdtd_face {
+  int32_t thickness;      /* PML layers on this face, 0 = none                            */
+  int32_t pad_;
+  const double* param_e;  /* float64[3][thickness]: p0, p1, p2 of the E update (cpml_params) */
+  const double* param_h;  /* the same for the H update                                    */
+  void* psi_e[2];         /* psi of the E update, two transverse components, psi_type,     */
+  void* psi_h[2];         /* each of the face region's shape (thickness along the axis)    */
+} fdfd_fdtd_face;
+
+typedef struct fdfd_fdtd_desc {
+  int32_t shape[3];
+  int32_t field_type;     /* FDFD_REAL64 / FDFD_REAL32                                    */
+  int32_t psi_type;       /* FDFD_REAL64 / FDFD_REAL32 (updates_with_cpml's dtype)         */
+  int32_t form;           /* FDFD_FDTD_PLAIN / FDFD_FDTD_CPML                              */
+  double dt;
+  const double* dxe[3];   /* float64[shape[a]]: dxes[0][a]                                 */
+  const double* dxh[3];   /* float64[shape[a]]: dxes[1][a]                                 */
+  const double* epsilon;  /* float64[3N]                                                   */
+  const double* mu;       /* float64[3N] or NULL (mu = 1)                                  */
+  fdfd_fdtd_face face[3][2]; /* [axis][0: low face (polarity -1), 1: high face (+1)]      */
+} fdfd_fdtd_desc;
+
+/* H half step: maxwell_h(dt, dxes)(E, H, mu) or updates_with_cpml's update_H(E, H, mu). */
+int fdfd_fdtd_update_h(const fdfd_fdtd_desc* desc, const void* E, void* H, void* stream);
+/* E half step: maxwell_e(dt, dxes)(E, H, epsilon) or update_E(E, H, epsilon). */
+int fdfd_fdtd_update_e(const fdfd_fdtd_desc* desc, void* E, const void* H, void* stream);
+
 /* fdfd_residual without a workspace, for callers that cannot allocate device memory
  * (an exhausted or frozen allocator, or a host program that owns every device buffer
  * and can pass only inputs and outputs).  No counterpart in the reference.

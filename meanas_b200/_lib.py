@@ -79,6 +79,21 @@ class CsrDesc(C.Structure):  # fdfd_csr_desc
                 ('data', C.c_void_p)]
 
 
+class FdtdFace(C.Structure):  # fdfd_fdtd_face
+    _fields_ = [('thickness', C.c_int32), ('pad_', C.c_int32), ('param_e', C.c_void_p), ('param_h', C.c_void_p),
+                ('psi_e', C.c_void_p * 2), ('psi_h', C.c_void_p * 2)]
+
+
+class FdtdDesc(C.Structure):  # fdfd_fdtd_desc
+    _fields_ = [('shape', C.c_int32 * 3), ('field_type', C.c_int32), ('psi_type', C.c_int32), ('form', C.c_int32),
+                ('dt', C.c_double), ('dxe', C.c_void_p * 3), ('dxh', C.c_void_p * 3), ('epsilon', C.c_void_p),
+                ('mu', C.c_void_p), ('face', (FdtdFace * 2) * 3)]
+
+
+REAL64, REAL32 = 0, 1
+FDTD_PLAIN, FDTD_CPML = 0, 1
+
+
 EXPORTS = {
     'fdfd_abi_version': (C.c_int, []),
     'fdfd_last_error': (C.c_char_p, []),
@@ -102,6 +117,8 @@ EXPORTS = {
     'fdfd_csr_solve_workspace_bytes': (C.c_int, [C.POINTER(CsrDesc), C.POINTER(C.c_size_t)]),
     'fdfd_csr_solve': (C.c_int, [C.POINTER(CsrDesc), C.POINTER(SolveOpts), C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.c_size_t, C.POINTER(SolveInfo), C.c_void_p]),
+    'fdfd_fdtd_update_h': (C.c_int, [C.POINTER(FdtdDesc), C.c_void_p, C.c_void_p, C.c_void_p]),
+    'fdfd_fdtd_update_e': (C.c_int, [C.POINTER(FdtdDesc), C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 # fdfd_tfsf_source flags

@@ -14,7 +14,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 LIB = HERE / 'libmeanas_fdfd.so'
 SOURCES = [HERE / 'csrc' / 'fdfd_lib.cu']
-DEPS = SOURCES + [HERE / 'csrc' / 'fdfd_device.cuh', HERE / 'csrc' / 'fdfd_ops.cuh', HERE / 'csrc' / 'fdfd_csr.cuh',
+DEPS = SOURCES + [HERE / 'csrc' / 'fdfd_device.cuh', HERE / 'csrc' / 'fdfd_ops.cuh', HERE / 'csrc' / 'fdfd_csr.cuh', HERE / 'csrc' / 'fdfd_fdtd.cuh',
                   HERE.parent / 'include' / 'meanas_fdfd.h']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 

@@ -15,6 +15,7 @@
 
 #include "../../include/meanas_fdfd.h"
 #include "fdfd_csr.cuh"
+#include "fdfd_fdtd.cuh"
 #include "fdfd_ops.cuh"
 
 using namespace fdfd;
@@ -1221,6 +1222,84 @@ extern "C" int fdfd_csr_solve(const fdfd_csr_desc* d, const fdfd_solve_opts* o, 
     info->residual_pc = info->residual;
   }
   return status == ST_CONVERGED ? 0 : status;
+}
+
+// ------------------------------------------------------------------ FDTD
+static int fdtd_geo(const fdfd_fdtd_desc* d, bool estep, FdtdGeo* g, const char* who) {
+  if (!d) return set_err(FDFD_ERR_ARG, "%s: NULL descriptor", who);
+  for (int a = 0; a < 3; ++a) {
+    if (d->shape[a] < 1) return set_err(FDFD_ERR_ARG, "%s: shape[%d] = %d", who, a, d->shape[a]);
+    if (!d->dxe[a] || !d->dxh[a]) return set_err(FDFD_ERR_ARG, "%s: NULL cell widths", who);
+  }
+  const long long n = (long long)d->shape[0] * d->shape[1] * d->shape[2];
+  if (3 * n >= (1LL << 31)) return set_err(FDFD_ERR_ARG, "%s: grid too large for 32-bit indexing", who);
+  if ((d->field_type != FDFD_REAL64 && d->field_type != FDFD_REAL32) ||
+      (d->psi_type != FDFD_REAL64 && d->psi_type != FDFD_REAL32))
+    return set_err(FDFD_ERR_ARG, "%s: bad field or psi type", who);
+  if (d->form != FDFD_FDTD_PLAIN && d->form != FDFD_FDTD_CPML) return set_err(FDFD_ERR_ARG, "%s: bad form", who);
+  if (estep && !d->epsilon) return set_err(FDFD_ERR_ARG, "%s: epsilon is NULL", who);
+  *g = FdtdGeo{};
+  g->X = d->shape[0];
+  g->Y = d->shape[1];
+  g->Z = d->shape[2];
+  g->ntz = (g->Z + 31) / 32;
+  g->nty = (g->Y + 7) / 8;
+  for (int a = 0; a < 3; ++a) {
+    g->dxb[a] = d->dxh[a];
+    g->dxf[a] = d->form == FDFD_FDTD_PLAIN ? d->dxe[a] : d->dxh[a];
+  }
+  g->mat = estep ? d->epsilon : d->mu;
+  g->dt = d->dt;
+  g->cpml = d->form == FDFD_FDTD_CPML;
+  if (g->cpml) {
+    for (int a = 0; a < 3; ++a) {
+      for (int pp = 0; pp < 2; ++pp) {
+        const fdfd_fdtd_face& f = d->face[a][pp];
+        if (f.thickness == 0) continue;
+        if (f.thickness < 0 || f.thickness > d->shape[a])
+          return set_err(FDFD_ERR_ARG, "%s: face [%d][%d] thickness %d", who, a, pp, f.thickness);
+        const double* par = estep ? f.param_e : f.param_h;
+        void* const* psi = estep ? f.psi_e : f.psi_h;
+        if (!par || !psi[0] || !psi[1]) return set_err(FDFD_ERR_ARG, "%s: face [%d][%d] NULL arrays", who, a, pp);
+        g->face[a][pp] = CpmlFace{f.thickness, par, psi[0], psi[1]};
+      }
+    }
+  }
+  return 0;
+}
+
+template <typename R, typename P, bool ESTEP>
+static int fdtd_launch(const FdtdGeo& g, void* e, void* h, cudaStream_t s) {
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  auto kern = k_fdtd<R, P, ESTEP>;
+  static const int occ = occupancy(kern, 256);
+  const long long units = (long long)g.ntz * g.nty * g.X;
+  kern<<<(unsigned)std::min(units, (long long)occ * nsm), dim3(32, 8), 0, s>>>(g, (R*)e, (R*)h);
+  CKL();
+  return 0;
+}
+
+template <bool ESTEP>
+static int fdtd_step(const fdfd_fdtd_desc* d, void* e, void* h, void* stream, const char* who) {
+  FdtdGeo g;
+  TRY(fdtd_geo(d, ESTEP, &g, who));
+  if (!e || !h) return set_err(FDFD_ERR_ARG, "%s: NULL field", who);
+  cudaStream_t s = (cudaStream_t)stream;
+  const bool f32 = d->field_type == FDFD_REAL32, p32 = d->psi_type == FDFD_REAL32;
+  if (f32 && p32) return fdtd_launch<float, float, ESTEP>(g, e, h, s);
+  if (f32) return fdtd_launch<float, double, ESTEP>(g, e, h, s);
+  if (p32) return fdtd_launch<double, float, ESTEP>(g, e, h, s);
+  return fdtd_launch<double, double, ESTEP>(g, e, h, s);
+}
+
+extern "C" int fdfd_fdtd_update_h(const fdfd_fdtd_desc* d, const void* E, void* H, void* stream) {
+  return fdtd_step<false>(d, const_cast<void*>(E), H, stream, "fdfd_fdtd_update_h");
+}
+
+extern "C" int fdfd_fdtd_update_e(const fdfd_fdtd_desc* d, void* E, const void* H, void* stream) {
+  return fdtd_step<true>(d, E, const_cast<void*>(H), stream, "fdfd_fdtd_update_e");
 }
 
 // ------------------------------------------------------------------ allocation-free residual

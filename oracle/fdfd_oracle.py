@@ -37,6 +37,10 @@ What each function restates:
   (``meanas/fdfd/operators.py:366-393``) and, with ``edges``, the edge mask of
   ``e_boundary_source`` (``:396-450``; mirrored or periodic one-cell shifts,
   ``meanas/fdmath/operators.py:55-98``).
+* ``fdtd_plain_step`` / ``CpmlUpdates``  the FDTD Yee updates: ``maxwell_h`` /
+  ``maxwell_e`` (``meanas/fdtd/base.py:13-125``) and ``updates_with_cpml``
+  (``meanas/fdtd/pml.py:115-230``, which divides its forward differences by the H-grid
+  widths ``dxes[1]``) with psi and the PML sums held in the psi dtype, as there.
 * ``cocg``           complex-symmetric CG in the E-space with the ``p^2``-weighted
   bilinear form: algebraically the COCG iteration on ``Pl A0 Pr`` (the system
   ``generic()`` builds) rewritten with ``x = Pl E``; the GPU solver runs the same
@@ -158,6 +162,88 @@ def tfsf_source(omega, dxes, epsilon, E, tf_region, mu=None, *, edges=False, per
         shape = _shape_of(dxes)
         j = j * _edge_mask(q.reshape(3, *shape), periodic).ravel()
     return j
+
+
+def fdtd_plain_step(e: NDArray, h: NDArray, epsilon: NDArray, dt: float, dxes) -> None:
+    """One ``maxwell_h`` then ``maxwell_e`` update of (3,X,Y,Z) fields, in place."""
+    h -= dt * curl_forward(dxes[0], e)
+    e += dt * curl_back(dxes[1], h) / epsilon
+
+
+class CpmlUpdates:
+    """``updates_with_cpml``: ``update_E(e, h, epsilon)`` / ``update_H(e, h, mu)`` in place.
+    ``params[axis][pp]`` is None or ``(param_e, param_h)`` with each a (3, th) array of
+    ``p0, p1, p2`` per layer (``pp = 0``: the low face, ``1``: the high face)."""
+
+    def __init__(self, params, dt: float, dxes, shape, dtype=numpy.float32):
+        self.dt = dt
+        self.dx = [numpy.asarray(d, dtype=float) for d in dxes[1]]
+        self.shape = tuple(shape)
+        self.dtype = dtype
+        self.params = params
+        self.psi_e = [[None, None] for _ in range(3)]
+        self.psi_h = [[None, None] for _ in range(3)]
+        for a in range(3):
+            for pp in range(2):
+                if params[a][pp] is not None:
+                    th = params[a][pp][0].shape[1]
+                    rs = list(self.shape)
+                    rs[a] = th
+                    self.psi_e[a][pp] = [numpy.zeros(rs, dtype) for _ in range(2)]
+                    self.psi_h[a][pp] = [numpy.zeros(rs, dtype) for _ in range(2)]
+
+    def _region(self, a, pp, th):
+        sl = [slice(None)] * 3
+        sl[a] = slice(None, th) if pp == 0 else slice(-th, None)
+        return tuple(sl)
+
+    def _bcast(self, v, a):
+        idx = [None, None, None]
+        idx[a] = slice(None)
+        return v[tuple(idx)]
+
+    def _pml(self, d, psi, side):
+        p = numpy.zeros((3, *self.shape), dtype=self.dtype)
+        for a in range(3):
+            se = (-1, 1, -1)[a]
+            u, v = [b for b in range(3) if b != a]
+            du, dv = d[a]
+            for pp in range(2):
+                if self.params[a][pp] is None:
+                    continue
+                tab = self.params[a][pp][0 if side == 'e' else 1]
+                p0, p1, p2 = (self._bcast(tab[i], a) for i in range(3))
+                reg = self._region(a, pp, tab.shape[1])
+                du[reg] *= p2
+                dv[reg] *= p2
+                pu, pv = psi[a][pp]
+                pu *= p0
+                pv *= p0
+                pu += p1 * dv[reg]
+                pv += p1 * du[reg]
+                p[u][reg] += +se * pu
+                p[v][reg] += -se * pv
+        return p
+
+    def update_E(self, e, h, epsilon):
+        b = [lambda f, a=a: (f - numpy.roll(f, 1, axis=a)) / self._bcast(self.dx[a], a) for a in range(3)]
+        dyHx, dzHx = b[1](h[0]), b[2](h[0])
+        dxHy, dzHy = b[0](h[1]), b[2](h[1])
+        dxHz, dyHz = b[0](h[2]), b[1](h[2])
+        p = self._pml(((dxHy, dxHz), (dyHx, dyHz), (dzHx, dzHy)), self.psi_e, 'e')
+        e[0] += self.dt / epsilon[0] * (dyHz - dzHy + p[0])
+        e[1] += self.dt / epsilon[1] * (dzHx - dxHz + p[1])
+        e[2] += self.dt / epsilon[2] * (dxHy - dyHx + p[2])
+
+    def update_H(self, e, h, mu=(1, 1, 1)):
+        f = [lambda g, a=a: (numpy.roll(g, -1, axis=a) - g) / self._bcast(self.dx[a], a) for a in range(3)]
+        dyEx, dzEx = f[1](e[0]), f[2](e[0])
+        dxEy, dzEy = f[0](e[1]), f[2](e[1])
+        dxEz, dyEz = f[0](e[2]), f[1](e[2])
+        p = self._pml(((dxEy, dxEz), (dyEx, dyEz), (dzEx, dzEy)), self.psi_h, 'h')
+        h[0] -= self.dt / mu[0] * (dyEz - dzEy + p[0])
+        h[1] -= self.dt / mu[1] * (dzEx - dxEz + p[1])
+        h[2] -= self.dt / mu[2] * (dxEy - dyEx + p[2])
 
 
 def precond_p2(dxes) -> NDArray:

@@ -23,6 +23,11 @@ the only place that reads it.  Outputs:
 * ``sources.npz``   ``operators.e_tfsf_source(Q, ...) @ x`` and
                     ``operators.e_boundary_source(Q, ..., periodic_mask_edges) @ x`` for
                     box-shaped and random total-field regions.
+* ``fdtd.npz``      reference FDTD trajectories: ``maxwell_h`` / ``maxwell_e`` steps with a
+                    current injected at steps 0, 4, 8 (the loop of
+                    ``meanas/test/test_fdtd.py:203-235``), and ``updates_with_cpml`` with
+                    ``cpml_params`` on every face (float32 and float64 fields), plus the
+                    CPML parameter tables.
 * ``dipole48.npz``  reference ``generic()`` on the 48^3 dipole-in-core problem
                     (rtol 1e-8, scipy QMR): field stored as complex64.
 """
@@ -40,6 +45,7 @@ sys.path.insert(0, str(Path(__file__).resolve().parents[2]))
 
 import scipy.sparse  # noqa: E402
 from meanas.fdfd import functional, operators, scpml, solvers, waveguide_3d  # noqa: E402
+from meanas import fdtd  # noqa: E402
 from meanas.fdmath import vec, unvec  # noqa: E402
 
 # generic(adjoint=True) uses csr_array.H, which SciPy >= 1.14 removed.
@@ -210,6 +216,96 @@ def gen_sources() -> None:
     numpy.savez_compressed(OUT / 'sources.npz', **out)
 
 
+def gen_fdtd() -> None:
+    rng = numpy.random.default_rng(99)
+    out = {}
+    n = 0
+    # plain Yee updates (maxwell_h then maxwell_e, current added at steps 0, 4, 8)
+    for shape, dt, kind in (((5, 5, 1), 0.3, 'center'), ((6, 7, 5), 0.3, 'random'), ((9, 4, 6), 0.25, 'random')):
+        f3 = (3, *shape)
+        dxes = [[numpy.full(s, 1.5) for s in shape] for _ in range(2)]
+        for g in range(2):
+            for a in range(3):
+                dxes[g][a][dxes[g][a].size // 2] *= 1.1
+        eps = rng.uniform(1.0, 2.5, f3)
+        j = numpy.zeros(f3)
+        if kind == 'center':
+            j[:, shape[0] // 2, shape[1] // 2, shape[2] // 2] = 1.0
+        else:
+            j[:] = rng.uniform(-1, 1, f3)
+        e = numpy.zeros(f3)
+        h = numpy.zeros(f3)
+        eh2h = fdtd.maxwell_h(dt=dt, dxes=dxes)
+        eh2e = fdtd.maxwell_e(dt=dt, dxes=dxes)
+        es, hs = [], []
+        for tt in range(10):
+            e = e.copy()
+            h = h.copy()
+            eh2h(e, h)
+            eh2e(e, h, eps)
+            if tt in (0, 4, 8):
+                e += j / eps
+            es.append(e)
+            hs.append(h)
+        p = f'c{n}_'
+        out[p + 'kind'] = numpy.array('plain')
+        out[p + 'shape'] = numpy.array(shape)
+        out[p + 'dt'] = numpy.array(dt)
+        for g in range(2):
+            for a in range(3):
+                out[f'{p}dx{g}{a}'] = dxes[g][a]
+        out[p + 'eps'] = eps
+        out[p + 'j'] = j
+        out[p + 'es'] = numpy.array(es)
+        out[p + 'hs'] = numpy.array(hs)
+        n += 1
+    # CPML updates on all six faces
+    for shape, dt, th, ftype in (((20, 16, 14), 0.3, 4, numpy.float32), ((12, 18, 1), 0.3, 5, numpy.float64),
+                                 ((16, 12, 22), 0.25, 6, numpy.float64)):
+        f3 = (3, *shape)
+        dxes = [[rng.uniform(0.9, 1.1, s) for s in shape] for _ in range(2)]
+        eps = rng.uniform(1.0, 4.0, f3)
+        params = [[None, None] for _ in range(3)]
+        for a in range(3):
+            if shape[a] > 2 * th:
+                for pp, pol in enumerate((-1, 1)):
+                    params[a][pp] = fdtd.cpml_params(axis=a, polarity=pol, dt=dt, thickness=th,
+                                                     epsilon_eff=1.5, cfs_alpha=0.05)
+        upd_e, upd_h = fdtd.updates_with_cpml(cpml_params=params, dt=dt, dxes=dxes, epsilon=eps, dtype=numpy.float32)
+        e = numpy.zeros(f3, dtype=ftype)
+        h = numpy.zeros(f3, dtype=ftype)
+        src = tuple(s // 2 for s in shape)
+        es, hs = [], []
+        for tt in range(40):
+            upd_h(e, h)
+            upd_e(e, h, eps)
+            e[(2, *src)] += numpy.sin(0.35 * tt) * numpy.exp(-((tt - 12) / 6) ** 2)
+            if tt % 8 == 7:
+                es.append(e.copy())
+                hs.append(h.copy())
+        p = f'c{n}_'
+        out[p + 'kind'] = numpy.array('cpml')
+        out[p + 'shape'] = numpy.array(shape)
+        out[p + 'dt'] = numpy.array(dt)
+        out[p + 'th'] = numpy.array(th)
+        out[p + 'ftype'] = numpy.array(numpy.dtype(ftype).name)
+        for g in range(2):
+            for a in range(3):
+                out[f'{p}dx{g}{a}'] = dxes[g][a]
+        out[p + 'eps'] = eps
+        out[p + 'es'] = numpy.array(es)
+        out[p + 'hs'] = numpy.array(hs)
+        for a in range(3):
+            for pp in range(2):
+                if params[a][pp] is not None:
+                    for side in ('e', 'h'):
+                        tab = numpy.stack([numpy.ravel(v) for v in params[a][pp]['param_' + side]])
+                        out[f'{p}pml{a}{pp}{side}'] = tab
+        n += 1
+    out['n'] = numpy.array(n)
+    numpy.savez_compressed(OUT / 'fdtd.npz', **out)
+
+
 def gen_solve() -> None:
     """Reference generic() solutions."""
     rng = numpy.random.RandomState(12345)
@@ -348,7 +444,7 @@ def gen_dipole48() -> None:
 
 
 if __name__ == '__main__':
-    which = sys.argv[2:] or ['scpml', 'operator', 'e2h', 'sources', 'solve', 'dipole48']
+    which = sys.argv[2:] or ['scpml', 'operator', 'e2h', 'sources', 'fdtd', 'solve', 'dipole48']
     for w in which:
         t = time.perf_counter()
         globals()[f'gen_{w}']()
