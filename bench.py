@@ -421,6 +421,27 @@ def kernel_mode(args) -> None:
     # CSR product of the matrix_solver hook on a matrix shaped like the assembled operator:
     # 3N rows, 13 nonzeros per row at the curl-curl stencil's column offsets (synthetic
     # values); bytes = values + column indices + row pointers + x once + y
+    # FDTD: one H + one E half step of the plain Yee updates on float32 fields (E step: read
+    # H, E, epsilon (float64), write E = 60 B/cell; H step: read E, H, write H = 36 B/cell)
+    from meanas_b200 import fdtd
+    rdx = [[numpy.abs(d).astype(float) for d in g] for g in p.dxes]
+    eh2h, eh2e = fdtd.maxwell_h(0.3, rdx, device=dev), fdtd.maxwell_e(0.3, rdx, device=dev)
+    ef = torch.randn((3, *p.shape), dtype=torch.float32, device=dev)
+    hf = torch.randn_like(ef)
+    epsf = torch.as_tensor(p.epsilon, device=dev)
+    for _ in range(3):
+        eh2h(ef, hf)
+        eh2e(ef, hf, epsf)
+    a.record()
+    for _ in range(10):
+        eh2h(ef, hf)
+        eh2e(ef, hf, epsf)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / 10
+    print(f'fdtd   H+E step f32                10 steps     {ms * 1e3:8.1f} us  '
+          f'{96 * p.n_cells / (ms / 1e3) / 1e9:7.1f} GB/s algorithmic')
+    del ef, hf
     if p.n_unknowns > 12_000_000:
         return
     from scipy import sparse
