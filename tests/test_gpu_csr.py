@@ -57,8 +57,12 @@ def test_solve_matches_direct_solution(cuda, n):
     M = CsrMatrix(A, cuda)
     x, info = M.solve(b, rtol=1e-12)
     assert info['status'] == 'converged', info
-    ref = scipy.sparse.linalg.spsolve(A.tocsc(), b)
-    assert numpy.linalg.norm(x.cpu().numpy() - ref) <= 1e-10 * numpy.linalg.norm(ref)
+    xh = x.cpu().numpy()
+    if n <= 1000:  # a direct solve of a random sparsity pattern fills in: small n only
+        ref = scipy.sparse.linalg.spsolve(A.tocsc(), b)
+        assert numpy.linalg.norm(xh - ref) <= 1e-10 * numpy.linalg.norm(ref)
+    # the true residual, recomputed on the host
+    assert numpy.linalg.norm(A @ xh - b) <= 1.01e-12 * numpy.linalg.norm(b)
     assert info['residual'] <= 1e-12 * 1.01
     # warm start from the answer: converged before the first iteration
     x2, info2 = M.solve(b, x.cpu().numpy(), rtol=1e-10)
