@@ -213,10 +213,10 @@ def run_ours(args) -> dict | None:
         return max_over_ranks(total_ms, world), lats, infos
 
     # Per-kernel CUDA-event timing inside the timed solves costs two event records per launch
-    # and disables the iteration graphs: negligible against ~0.3 ms iterations (large grids),
-    # not against 20 us ones.  Small grids time graph-launched solves for `value` and take the
-    # kernel durations from one extra profiled solve per method.
-    live = args.timed_profile == 'on' or (args.timed_profile == 'auto' and ncell >= 2_000_000)
+    # and disables the iteration graphs (about 10 % at 160x160x128, far more on small grids),
+    # so the timed solves run as they do in production (graph launches) and the kernel
+    # durations of the roofline come from one profiled solve per method right after them.
+    live = args.timed_profile == 'on'
     out = {}
     with Clocks(local) as clk:
         for method in args.methods.split(','):
@@ -587,8 +587,9 @@ def main():
     ap.add_argument('--kernel-iters', type=int, default=0,
                     help='profiling mode: run this many iterations of each solver (no convergence, no JSON)')
     ap.add_argument('--shape', type=int, nargs=3, default=None, help='profiling mode grid shape')
-    ap.add_argument('--timed-profile', choices=['auto', 'on', 'off'], default='auto',
-                    help='per-launch CUDA events inside the timed solves (auto: grids of >= 2M cells)')
+    ap.add_argument('--timed-profile', choices=['on', 'off'], default='off',
+                    help='per-launch CUDA events inside the timed solves (off: graph launches, kernel '
+                         'durations from one profiled solve after them)')
     ap.add_argument('--maxiter', type=int, default=None,
                     help='cap the Krylov iterations of each timed solve (measurement runs; reports the status)')
     ap.add_argument('--gradient-check', action='store_true', help='adjoint gradient vs finite differences')
