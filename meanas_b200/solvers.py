@@ -20,7 +20,9 @@ Differences from the reference, all deliberate:
   A ``callback`` cannot run per iteration on the device; it is called once with
   the final iterate of the symmetrised system.
 * A custom ``matrix_solver`` (which expects an assembled CSR matrix) is not
-  supported and raises ``NotImplementedError``.
+  supported here and raises ``NotImplementedError``; to keep the reference's CSR flow
+  and still solve on the GPU, pass ``meanas_b200.csr.matrix_solver`` to the reference's
+  own ``generic()``.
 * Non-convergence is not silent: it logs a WARNING, and the outcome of the last
   call is available from :func:`last_solve_info` (or ``return_info=True``).
 * The adjoint path works on current SciPy (the reference's ``.H`` on
@@ -84,8 +86,9 @@ def generic(
     """
     global _LAST_INFO
     if matrix_solver is not None:
-        raise NotImplementedError('meanas_b200.generic runs its own matrix-free GPU solver; '
-                                  'a CSR matrix_solver cannot be plugged in')
+        raise NotImplementedError('meanas_b200.generic runs its own matrix-free GPU solver; a CSR '
+                                  'matrix_solver cannot be plugged in (for the CSR flow, pass '
+                                  'meanas_b200.csr.matrix_solver to meanas.fdfd.solvers.generic)')
     opts = dict(matrix_solver_opts or {})
     rtol = float(opts.pop('rtol', 1e-5))
     atol = float(opts.pop('atol', 0.0))
