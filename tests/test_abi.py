@@ -93,3 +93,27 @@ def test_no_cpu_fallback_in_product_package():
     for p in (ROOT / 'meanas_b200').rglob('*.py'):
         text = p.read_text()
         assert 'from oracle' not in text and 'import oracle' not in text, p
+
+
+def test_fdtd_argument_checks_need_no_gpu():
+    from meanas_b200 import _lib
+    lib = _lib.load()
+    d = _lib.FdtdDesc()
+    d.shape[:] = (4, 0, 4)
+    assert lib.fdfd_fdtd_update_h(C.byref(d), 1, 1, None) == -1
+    assert b'shape[1]' in lib.fdfd_last_error()
+    d.shape[:] = (4, 4, 4)
+    for a in range(3):
+        d.dxe[a] = d.dxh[a] = 1  # any non-NULL pointer: only the checks run
+    d.field_type = 7
+    assert lib.fdfd_fdtd_update_h(C.byref(d), 1, 1, None) == -1
+    assert b'type' in lib.fdfd_last_error()
+    d.field_type = _lib.REAL32
+    assert lib.fdfd_fdtd_update_e(C.byref(d), 1, 1, None) == -1   # E step needs epsilon
+    assert b'epsilon' in lib.fdfd_last_error()
+    d.form = _lib.FDTD_CPML
+    d.epsilon = 1
+    d.face[0][0].thickness = 9                                      # thicker than the axis
+    d.face[0][0].param_e = d.face[0][0].param_h = 1
+    assert lib.fdfd_fdtd_update_e(C.byref(d), 1, 1, None) == -1
+    assert b'thickness' in lib.fdfd_last_error()
