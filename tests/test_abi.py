@@ -99,12 +99,15 @@ def test_fdtd_argument_checks_need_no_gpu():
     from meanas_b200 import _lib
     lib = _lib.load()
     d = _lib.FdtdDesc()
+    d.shape[:] = (4, 4, 4)
+    assert lib.fdfd_fdtd_update_h(C.byref(d), 1, 1, None) == -1
+    assert b'cell widths' in lib.fdfd_last_error()
+    for a in range(3):
+        d.dxe[a] = d.dxh[a] = 1  # any non-NULL pointer: only the checks run
     d.shape[:] = (4, 0, 4)
     assert lib.fdfd_fdtd_update_h(C.byref(d), 1, 1, None) == -1
     assert b'shape[1]' in lib.fdfd_last_error()
     d.shape[:] = (4, 4, 4)
-    for a in range(3):
-        d.dxe[a] = d.dxh[a] = 1  # any non-NULL pointer: only the checks run
     d.field_type = 7
     assert lib.fdfd_fdtd_update_h(C.byref(d), 1, 1, None) == -1
     assert b'type' in lib.fdfd_last_error()
