@@ -31,7 +31,6 @@ struct CpmlFace {
 struct FdtdGeo {
   int X, Y, Z;
   int ntz, nty;
-  int XC, nxc;            // x planes per CTA, x chunks
   const double* dxf[3];   // widths dividing the forward differences
   const double* dxb[3];   // widths dividing the backward differences
   const double* mat;      // epsilon (E step) or mu (H step, may be null: 1), [3N]
@@ -73,74 +72,46 @@ __device__ __forceinline__ P psi_step(P psi, double p0, double p1, double d) {
   return (P)dadd((double)a, dmulr(p1, d));
 }
 
-// One half step on every cell: ESTEP updates E from H, otherwise H from E.  A CTA owns a
-// 32(z) x 8(y) tile and marches along x over a chunk of planes; the two components whose
-// x difference needs the neighbouring plane are carried in registers from one plane to
-// the next (E step: H of plane i-1; H step: E of plane i+1 becomes plane i's own), so
-// each cell loads 7 values of the other field instead of 9.
+// One half step on every cell: ESTEP updates E from H, otherwise H from E.
 template <typename R, typename P, bool ESTEP>
-__global__ void __launch_bounds__(256, 4) k_fdtd(FdtdGeo g, R* __restrict__ e, R* __restrict__ h) {
-  int b = blockIdx.x;
-  const int tzb = b % g.ntz;
-  b /= g.ntz;
-  const int tyb = b % g.nty;
-  const int xcb = b / g.nty;
-  const int j = tyb * 8 + threadIdx.y, k = tzb * 32 + threadIdx.x;
-  if (j >= g.Y || k >= g.Z) return;  // no CTA barriers in this kernel
-  const int x0 = xcb * g.XC, x1 = min(g.X, x0 + g.XC);
+__global__ void __launch_bounds__(256) k_fdtd(FdtdGeo g, R* __restrict__ e, R* __restrict__ h) {
+  const int ntiles = g.ntz * g.nty, units = ntiles * g.X;
   const int YZ = g.Y * g.Z, N = g.X * YZ;
-  const int jn = ESTEP ? (j == 0 ? g.Y - 1 : j - 1) : (j + 1 == g.Y ? 0 : j + 1);
-  const int kn = ESTEP ? (k == 0 ? g.Z - 1 : k - 1) : (k + 1 == g.Z ? 0 : k + 1);
-  const int oy = (jn - j) * g.Z, oz = kn - k;
-  const double wy = ESTEP ? g.dxb[1][j] : g.dxf[1][j];
-  const double wz = ESTEP ? g.dxb[2][k] : g.dxf[2][k];
-  const R* src = ESTEP ? h : e;
-  R* dst = ESTEP ? e : h;
-  const int jk = j * g.Z + k;
-  // carried components 1 and 2 of the source field: E step, plane i-1; H step, plane i
-  R cy, cz;
-  {
-    const int ic = ESTEP ? (x0 == 0 ? g.X - 1 : x0 - 1) : x0;
-    cy = src[N + ic * YZ + jk];
-    cz = src[2 * N + ic * YZ + jk];
-  }
-  for (int i = x0; i < x1; ++i) {
-    const int c0 = i * YZ + jk;
+  for (int u = blockIdx.x; u < units; u += gridDim.x) {
+    const int i = u / ntiles, t = u - i * ntiles;
+    const int tyb = t / g.ntz, tzb = t - tyb * g.ntz;
+    const int j = tyb * 8 + threadIdx.y, k = tzb * 32 + threadIdx.x;
+    if (j >= g.Y || k >= g.Z) continue;
+    const int c0 = i * YZ + j * g.Z + k;
+    const int idx[3] = {i, j, k};
+    // neighbour cells: -1 (E step) or +1 (H step) along each axis, periodic
+    int nb[3];
+    if (ESTEP) {
+      nb[0] = c0 + ((i == 0 ? g.X - 1 : i - 1) - i) * YZ;
+      nb[1] = c0 + ((j == 0 ? g.Y - 1 : j - 1) - j) * g.Z;
+      nb[2] = c0 + ((k == 0 ? g.Z - 1 : k - 1) - k);
+    } else {
+      nb[0] = c0 + ((i + 1 == g.X ? 0 : i + 1) - i) * YZ;
+      nb[1] = c0 + ((j + 1 == g.Y ? 0 : j + 1) - j) * g.Z;
+      nb[2] = c0 + ((k + 1 == g.Z ? 0 : k + 1) - k);
+    }
+    const R* src = ESTEP ? h : e;
     // d[a][c]: difference along axis a of component c (only c != a is used)
     double d[3][3];
-    const double wx = ESTEP ? g.dxb[0][i] : g.dxf[0][i];
-    R s0, s1, s2;  // the source field at the own cell
-    if (ESTEP) {
-      s0 = src[c0];
-      s1 = src[N + c0];
-      s2 = src[2 * N + c0];
-      d[0][1] = ddivr((double)tsub<R>(s1, cy), wx);
-      d[0][2] = ddivr((double)tsub<R>(s2, cz), wx);
-      d[1][0] = ddivr((double)tsub<R>(s0, src[c0 + oy]), wy);
-      d[1][2] = ddivr((double)tsub<R>(s2, src[2 * N + c0 + oy]), wy);
-      d[2][0] = ddivr((double)tsub<R>(s0, src[c0 + oz]), wz);
-      d[2][1] = ddivr((double)tsub<R>(s1, src[N + c0 + oz]), wz);
-      cy = s1;
-      cz = s2;
-    } else {
-      const int cx1 = (i + 1 == g.X ? 0 : i + 1) * YZ + jk;
-      s0 = src[c0];
-      s1 = cy;
-      s2 = cz;
-      const R ny = src[N + cx1], nz = src[2 * N + cx1];
-      d[0][1] = ddivr((double)tsub<R>(ny, s1), wx);
-      d[0][2] = ddivr((double)tsub<R>(nz, s2), wx);
-      d[1][0] = ddivr((double)tsub<R>(src[c0 + oy], s0), wy);
-      d[1][2] = ddivr((double)tsub<R>(src[2 * N + c0 + oy], s2), wy);
-      d[2][0] = ddivr((double)tsub<R>(src[c0 + oz], s0), wz);
-      d[2][1] = ddivr((double)tsub<R>(src[N + c0 + oz], s1), wz);
-      cy = ny;
-      cz = nz;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double w = ESTEP ? g.dxb[a][idx[a]] : g.dxf[a][idx[a]];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        if (c == a) continue;
+        const R here = src[c * N + c0], there = src[c * N + nb[a]];
+        const R diff = ESTEP ? tsub<R>(here, there) : tsub<R>(there, here);
+        d[a][c] = ddivr((double)diff, w);
+      }
     }
     P pc[3] = {P(0), P(0), P(0)};
     if (g.cpml) {
       const int dims[3] = {g.X, g.Y, g.Z};
-      const int idx[3] = {i, j, k};
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         const int uu = a == 0 ? 1 : 0, vv = a == 2 ? 1 : 2;
@@ -175,6 +146,7 @@ __global__ void __launch_bounds__(256, 4) k_fdtd(FdtdGeo g, R* __restrict__ e, R
     curl[0] = dsub(d[1][2], d[2][1]);
     curl[1] = dsub(d[2][0], d[0][2]);
     curl[2] = dsub(d[0][1], d[1][0]);
+    R* dst = ESTEP ? e : h;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const R old = dst[c * N + c0];

@@ -1275,13 +1275,8 @@ static int fdtd_launch(const FdtdGeo& g, void* e, void* h, cudaStream_t s) {
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   auto kern = k_fdtd<R, P, ESTEP>;
   static const int occ = occupancy(kern, 256);
-  // x chunks: about two waves of CTAs over the resident slots
-  FdtdGeo gg = g;
-  const long long tiles = (long long)g.ntz * g.nty;
-  const long long want = 2LL * occ * nsm;
-  gg.XC = (int)std::max(1LL, std::min((long long)g.X, (g.X * tiles + want - 1) / want));
-  gg.nxc = (g.X + gg.XC - 1) / gg.XC;
-  kern<<<(unsigned)(tiles * gg.nxc), dim3(32, 8), 0, s>>>(gg, (R*)e, (R*)h);
+  const long long units = (long long)g.ntz * g.nty * g.X;
+  kern<<<(unsigned)std::min(units, (long long)occ * nsm), dim3(32, 8), 0, s>>>(g, (R*)e, (R*)h);
   CKL();
   return 0;
 }
