@@ -181,13 +181,14 @@ static void prof_collect(fdfd_plan* P, double* ms, int* cnt) {
 static constexpr int FLAT_TY = 256;
 
 // Resident CTAs per SM the stencil kernels are compiled for (register cap 65536 /
-// (256 threads x value)): complex64 passes carry less state than complex128 ones, and a
-// complex64 pass whose shared memory leaves room for four CTAs is given the registers of
-// four (the others would only lose registers without gaining residency).
-template <typename R, class Op>
+// (256 threads x value)): complex64 passes carry less state than complex128 ones.
+template <typename R>
 struct MinBlocks {
-  static constexpr size_t smem = StencilShape<R, 32, 8, false, Op::NB, Op::NO>::smem_bytes();
-  static constexpr int value = sizeof(R) == 8 ? 2 : ((smem + 1024) * 4 <= 228 * 1024 ? 4 : 3);
+  static constexpr int value = 2;
+};
+template <>
+struct MinBlocks<float> {
+  static constexpr int value = 3;
 };
 static constexpr int TZ3 = 32, TY3 = 8;
 
@@ -255,12 +256,12 @@ static int launch_stencil(fdfd_plan* P, const Geo<R>& g0, int precision, const O
   const Geo<R> g = geo_with(g0, t);
   if (P->flat) {
     using Sh = StencilShape<R, 1, FLAT_TY, true, Op::NB, Op::NO>;
-    auto kern = k_stencil<R, 1, FLAT_TY, true, MinBlocks<R, Op>::value, Op>;
+    auto kern = k_stencil<R, 1, FLAT_TY, true, MinBlocks<R>::value, Op>;
     ensure_smem(kern, Sh::smem_bytes());
     kern<<<(unsigned)t.nblocks, dim3(1, FLAT_TY), Sh::smem_bytes(), s>>>(g, op, rb);
   } else {
     using Sh = StencilShape<R, TZ3, TY3, false, Op::NB, Op::NO>;
-    auto kern = k_stencil<R, TZ3, TY3, false, MinBlocks<R, Op>::value, Op>;
+    auto kern = k_stencil<R, TZ3, TY3, false, MinBlocks<R>::value, Op>;
     ensure_smem(kern, Sh::smem_bytes());
     kern<<<(unsigned)t.nblocks, dim3(TZ3, TY3), Sh::smem_bytes(), s>>>(g, op, rb);
   }
