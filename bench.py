@@ -316,7 +316,19 @@ def run_ours(args) -> dict | None:
     return res
 
 
-def cpu_baseline(p, sample_iters: int, iters_full: int) -> dict:
+# Krylov iterations of one full solve of each workload, for extrapolating the CPU sample:
+# the reference's own QMR count where it was run (48^3: tests/golden/dipole48.npz), else
+# the GPU complex128 COCG count measured on a B200 (QMR and COCG build the same Krylov
+# space: 1189 vs 1192 iterations at 48^3); the masked case does not converge, so its cap.
+REF_ITERS = {
+    'dipole_core': (1189, 'the reference QMR count of this problem'),
+    'aniso_blocks': (50591, 'the GPU complex128 COCG count of this problem (the reference QMR took 1189 '
+                            'vs COCG 1192 on the 48^3 case)'),
+    'masked_large': (150000, 'the iteration cap of the unconverged GPU run of this problem'),
+}
+
+
+def cpu_baseline(p, sample_iters: int, iters_full: int, iters_source: str = '') -> dict:
     # (mu, PEC and PMC enter the CSR assembly like the reference's e_full)
     """Oracle port of the reference path timed on the host: assembly + `sample_iters`
     scipy QMR iterations, extrapolated to `iters_full` iterations per solve."""
@@ -333,11 +345,11 @@ def cpu_baseline(p, sample_iters: int, iters_full: int) -> dict:
     t2 = time.perf_counter()
     t_iter = (t2 - t1) / sample_iters
     t_solve = (t1 - t0) + iters_full * t_iter
-    return {'value': round(1.0 / t_solve, 6), 'unit': 'solves/s', 'cores': 1, 'kind': 'port',
+    return {'value': float(f'{1.0 / t_solve:.6g}'), 'unit': 'solves/s', 'cores': 1, 'kind': 'port',
             'sample': f'CSR assembly ({t1 - t0:.1f} s) + {sample_iters} scipy QMR iterations '
-                      f'({t_iter * 1e3:.0f} ms each) on the full {"x".join(map(str, p.shape))} system, extrapolated to '
-                      f'{iters_full} iterations (the GPU complex128 COCG count; the reference QMR took '
-                      f'1189 vs COCG 1192 on the 48^3 case)',
+                      f'({t_iter * 1e3:.0f} ms each; scipy\'s CSR product runs on one thread) on the full '
+                      f'{"x".join(map(str, p.shape))} system, extrapolated to {iters_full} iterations '
+                      f'({iters_source or "the GPU complex128 COCG count"})',
             'seconds_per_solve': round(t_solve, 1)}
 
 
@@ -348,9 +360,11 @@ def run_reference(args) -> dict | None:
     from meanas_b200 import workloads
     p = workloads.BY_NAME[args.workload]()
     samples = []
-    iters_full = args.ref_iters
+    iters_full, source = REF_ITERS[args.workload]
+    if args.ref_iters:
+        iters_full, source = args.ref_iters, 'given on the command line'
     for _ in range(args.warmup + args.steps):
-        samples.append(cpu_baseline(p, args.cpu_sample_iters, iters_full))
+        samples.append(cpu_baseline(p, args.cpu_sample_iters, iters_full, source))
     timed = samples[args.warmup:]
     v = statistics.median(s['value'] for s in timed)
     return {'metric': METRIC, 'value': v, 'unit': 'solves/s', 'n_gpus': args.gpus, 'steps': args.steps,
@@ -577,8 +591,9 @@ def main():
     ap.add_argument('--impl', choices=['ours', 'reference'], default='ours')
     ap.add_argument('--e2e-steps', type=int, default=2)
     ap.add_argument('--cpu-sample-iters', type=int, default=4)
-    ap.add_argument('--ref-iters', type=int, default=3000,
-                    help='QMR iterations per full solve used to extrapolate the reference arm')
+    ap.add_argument('--ref-iters', type=int, default=0,
+                    help='QMR iterations per full solve used to extrapolate the reference arm '
+                         '(0: the per-workload count in REF_ITERS)')
     ap.add_argument('--methods', default='mixed,cocg', help='GPU solvers to time (mixed, cocg)')
     ap.add_argument('--no-autotune', dest='autotune', action='store_false',
                     help='keep the default tiling instead of timing x-chunk candidates first')
