@@ -155,21 +155,31 @@ def dist_setup(n_gpus: int):
     return rank, world, local
 
 
+def _collective_device() -> str:
+    import torch
+    import torch.distributed as dist
+    return 'cuda' if dist.is_initialized() and dist.get_backend() == 'nccl' and torch.cuda.is_available() else 'cpu'
+
+
 def barrier_sync(world: int):
     import torch
     import torch.distributed as dist
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-        torch.cuda.synchronize()
+        if torch.cuda.is_available():
+            torch.cuda.synchronize()
 
 
 def max_over_ranks(v: float, world: int) -> float:
+    """The largest value over the ranks (every rank gets it): multi-GPU times are the slowest
+    rank's.  NCCL reduces on the device; a gloo group (CPU tests) on the host."""
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device='cuda')
+    t = torch.tensor([v], dtype=torch.float64, device=_collective_device())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
