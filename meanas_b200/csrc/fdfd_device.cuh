@@ -58,13 +58,6 @@ __device__ __forceinline__ cx<R> caxpy(cx<R> s, cx<R> b, cx<R> a) {
 template <typename R>
 __device__ __forceinline__ cx<R> czero() { return mkc<R>(R(0), R(0)); }
 
-template <typename R>
-__device__ __forceinline__ cx<R> cld(const cx<R>* p, int i) { return p[i]; }
-
-// Precision conversions.
-__device__ __forceinline__ cx<float> to_c64(cx<double> a) { return mkc<float>((float)a.re, (float)a.im); }
-__device__ __forceinline__ cx<double> to_c128(cx<float> a) { return mkc<double>((double)a.re, (double)a.im); }
-
 // FP64 complex scalars live in device memory as two doubles.
 struct dcx {
   double re, im;
