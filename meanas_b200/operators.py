@@ -323,7 +323,9 @@ class GridOperator:
                           max_outer=1)
                 self.solve(J, E_guess=guess, **kw)            # warm-up
                 _, info = self.solve(J, E_guess=guess, **kw)
-                n = max(1, info.kernel_count[kinds[0]])
+                # per real iteration: launches of a batch that starts after the cap return
+                # at once but are timed too, so divide by the iterations, not the launches
+                n = max(1, info.iterations)
                 timing[xc] = 1e3 * sum(info.kernel_ms[k] for k in kinds) / n
             xc = min(timing, key=timing.get)
             self.set_xchunk(prec, xc)
