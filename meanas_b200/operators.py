@@ -319,12 +319,13 @@ class GridOperator:
             timing = {}
             for xc in candidates:
                 self.set_xchunk(prec, xc)
+                # one batch of exactly `iters` iterations, so few no-op launches follow the cap
                 kw = dict(method=method, rtol=1e-30, maxiter=iters, criterion='true', profile=True,
-                          max_outer=1)
+                          max_outer=1, chunk=iters)
                 self.solve(J, E_guess=guess, **kw)            # warm-up
                 _, info = self.solve(J, E_guess=guess, **kw)
-                # per real iteration: launches of a batch that starts after the cap return
-                # at once but are timed too, so divide by the iterations, not the launches
+                # per real iteration (the no-op launches of the batch after the cap are timed
+                # too and add the same small amount to every candidate)
                 n = max(1, info.iterations)
                 timing[xc] = 1e3 * sum(info.kernel_ms[k] for k in kinds) / n
             xc = min(timing, key=timing.get)
