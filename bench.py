@@ -199,6 +199,8 @@ def run_ours(args) -> dict | None:
     stream = torch.cuda.current_stream()
     tuned = op.autotune(methods=tuple(args.methods.split(','))) if args.autotune else {}
 
+    fields = {}  # the last timed field of each method
+
     def timed(method: str, steps: int, warmup: int, profile: bool):
         kw = dict(method=method, rtol=RTOL, criterion='true', profile=profile, maxiter=args.maxiter)
         for _ in range(warmup):
@@ -212,8 +214,9 @@ def run_ours(args) -> dict | None:
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            _, info = op.solve(J, **kw)
+            E, info = op.solve(J, **kw)
             b.record(stream)
+            fields[method] = E
             infos.append(info)
             lat.append((a, b))
         t1.record(stream)
@@ -315,6 +318,7 @@ def run_ours(args) -> dict | None:
                      'timing': ('CUDA events around every launch of the timed solves' if live else
                                 'CUDA events around every launch of one profiled solve after the '
                                 'graph-launched timed solves')},
+        'field_rel_err': field_errors(fields, args.workload),
         'gpu_launches': int(b['launches']),
         'tiling': {k: {'xchunk': v[0], 'us_per_iteration': round(v[1], 1)} for k, v in tuned.items()},
         'clocks': clocks,
@@ -336,6 +340,26 @@ REF_ITERS = {
                             'vs COCG 1192 on the 48^3 case)'),
     'masked_large': (150000, 'the iteration cap of the unconverged GPU run of this problem'),
 }
+
+
+def field_errors(fields: dict, workload: str) -> dict:
+    """Relative field differences of the timed solves: the mixed-precision field against the
+    FP64 one, and on the 48^3 case each against the reference's own QMR field
+    (tests/golden/dipole48.npz, stored in complex64, so about 1e-7 is its floor)."""
+    import torch
+    out = {}
+    try:
+        if 'mixed' in fields and 'cocg' in fields:
+            a, b = fields['mixed'], fields['cocg']
+            out['mixed_vs_fp64'] = float((a - b).norm() / b.norm())
+        if workload == 'dipole_core' and fields:
+            ref = numpy.load(ROOT / 'tests' / 'golden' / 'dipole48.npz')['E'].astype(numpy.complex128)
+            r = torch.as_tensor(ref, device=next(iter(fields.values())).device)
+            for m, e in fields.items():
+                out[('fp64' if m == 'cocg' else m) + '_vs_reference_qmr'] = float((e - r).norm() / r.norm())
+    except Exception as exc:  # a report only: never a reason to lose the bench line
+        out['error'] = repr(exc)
+    return out
 
 
 def cpu_baseline(p, sample_iters: int, iters_full: int, iters_source: str = '') -> dict:
