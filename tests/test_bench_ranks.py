@@ -45,7 +45,7 @@ def _rank(rank: int, world: int, port: int, out) -> None:
 def test_two_gloo_ranks_agree_on_the_slowest_time():
     world = 2
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context('spawn').Manager() as m:  # no fork of this multi-threaded process
         out = m.dict()
         mp.spawn(_rank, args=(world, port, out), nprocs=world, join=True)
         assert [out[r] for r in range(world)] == [11.0, 11.0]
