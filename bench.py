@@ -57,7 +57,9 @@ def workload_config(name: str, p) -> dict:
                 l2=('inputs and per-iteration vectors larger than L2 (no flush)' if p.n_cells * 456 > 126e6
                     else 'working set fits in L2 (small reference case)'))
 RTOL = 1e-8
-# Algorithmic bytes per cell of each iteration kernel ("Kernels"):
+# Algorithmic bytes per cell of each iteration kernel (complex128 = 16 B, complex64 = 8 B
+# per component, eps 3 reals; the stencil's halo and neighbour-plane re-reads are served
+# from L2 and not counted):
 #   COCG stencil pass (c128): read r, p_old, x, eps; write p, x, q   = 6*48 + 24 = 312
 #   COCG pointwise pass (c128): read r, q; write r                  = 3*48      = 144
 #   BiCGSTAB P pass (c64): read r, v, t, p, x, eps; write r, p, v, x = 9*24 + 12 = 228
