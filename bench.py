@@ -577,7 +577,7 @@ def gradient_check(args) -> dict:
 
 
 def serving_run(args) -> dict:
-    """config[2]: a seeded Poisson stream of requests (sizes uniform over 128^2..1024^2 x1 and
+    """The serving stream: seeded Poisson arrivals of requests (sizes uniform over 128^2..1024^2 x1 and
     32^3..128^3, lambda ~ U[16, 40] cells, random eps blocks, one dipole each), mixed precision
     to a true FP64 residual of 1e-8, served with continuous batching."""
     import torch
