@@ -65,6 +65,7 @@ RTOL = 1e-8
 #   BiCGSTAB P pass (c64): read r, v, t, p, x, eps; write r, p, v, x = 9*24 + 12 = 228
 #   BiCGSTAB S pass (c64): read r, v, eps; write t                   = 3*24 + 12 = 84
 KERNEL_BYTES_PER_CELL = {0: 312, 1: 144, 2: 228, 3: 84}
+METHOD_NAMES = {'cocg': 'fp64 (complex128 COCG)', 'mixed': 'mixed (complex64 inner, complex128 refinement)'}
 KERNEL_NAMES = {0: 'cocg_stencil_c128', 1: 'cocg_point_c128', 2: 'bicgstab_P_c64', 3: 'bicgstab_S_c64'}
 
 
@@ -81,15 +82,19 @@ def peaks() -> tuple[float, str]:
 PROFILE_TAGS = {'aniso_blocks': 'aniso160', 'dipole_core': 'dipole48', 'masked_large': 'masked320'}
 
 
-def profile_traffic(kernel: str, workload: str) -> float | None:
-    """DRAM bytes per launch of `kernel` on `workload`, from the committed ncu summary
-    profiles/<kernel>_<workload tag>.md (None when that capture does not exist)."""
+def profile_traffic(kernel: str, workload: str) -> tuple[float | None, str | None]:
+    """DRAM bytes per launch of `kernel` on `workload` from the committed ncu summary
+    profiles/<kernel>_<workload tag>.md, and where that number comes from (the file and the
+    source commit it records for the capture).  (None, None) when no capture exists: ncu
+    cannot run inside the timed program, so the figure is the one of the last capture."""
     f = ROOT / 'profiles' / f'{kernel}_{PROFILE_TAGS[workload]}.md'
     if f.exists():
-        m = re.search(r'traffic_bytes_per_launch:\s*([0-9.eE+]+)', f.read_text())
+        text = f.read_text()
+        m = re.search(r'traffic_bytes_per_launch:\s*([0-9.eE+]+)', text)
         if m:
-            return float(m.group(1))
-    return None
+            c = re.search(r'captured_source_commit:\s*([0-9a-f]+)', text)
+            return float(m.group(1)), f'profiles/{f.name}' + (f' (capture of commit {c.group(1)})' if c else '')
+    return None, None
 
 
 class Clocks:
@@ -295,11 +300,12 @@ def run_ours(args) -> dict | None:
         extra_bytes = (3 * real if p.mu is not None else 0) + (1 if (p.pec is not None or p.pmc is not None) else 0)
     alg = (KERNEL_BYTES_PER_CELL[dom] + extra_bytes) * ncell
     achieved = alg / (avg_ms / 1e3) / 1e9
-    traffic = profile_traffic(KERNEL_NAMES[dom], args.workload)
+    traffic, traffic_source = profile_traffic(KERNEL_NAMES[dom], args.workload)
     share = b['kernel_ms'][dom] / b['prof_ms']
     steps_total = args.steps
     res = {
         'metric': METRIC, 'value': round(b['solves_per_s'], 4), 'unit': 'solves/s', 'n_gpus': world,
+        'value_method': METHOD_NAMES.get(best, best),
         'steps': steps_total, 'warmup': args.warmup, 'ms_per_step': round(b['ms_per_step'], 3),
         'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
         'dtype': 'c64 inner + c128 refinement' if best == 'mixed' else 'c128',
@@ -314,7 +320,7 @@ def run_ours(args) -> dict | None:
                             if 'mixed' in out and 'cocg' in out else None),
         'roofline': {'bound': 'hbm', 'kernel': KERNEL_NAMES[dom], 'achieved': round(achieved, 1),
                      'peak': peak, 'unit': 'GB/s', 'frac': round(achieved / peak, 4),
-                     'peak_kind': peak_kind, 'traffic': traffic,
+                     'peak_kind': peak_kind, 'traffic': traffic, 'traffic_source': traffic_source,
                      'algorithmic_bytes_per_launch': alg, 'avg_launch_ms': round(avg_ms, 5),
                      'share_of_step': round(share, 3),
                      'timing': ('CUDA events around every launch of the timed solves' if live else
@@ -364,11 +370,23 @@ def field_errors(fields: dict, workload: str) -> dict:
     return out
 
 
-def cpu_baseline(p, sample_iters: int, iters_full: int, iters_source: str = '') -> dict:
-    # (mu, PEC and PMC enter the CSR assembly like the reference's e_full)
-    """Oracle port of the reference path timed on the host: assembly + `sample_iters`
-    scipy QMR iterations, extrapolated to `iters_full` iterations per solve."""
-    import scipy.sparse.linalg
+def host_cpu() -> dict:
+    """The host's logical core count and CPU model (as /proc/cpuinfo names it)."""
+    model = None
+    try:
+        for line in Path('/proc/cpuinfo').read_text().splitlines():
+            if line.startswith('model name'):
+                model = line.split(':', 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {'nproc': os.cpu_count(), 'model': model}
+
+
+def reference_system(p):
+    """The system the reference's generic() hands to scipy's QMR, built by the oracle port:
+    CSR A0 (mu, PEC and PMC enter as in the reference's e_full), symmetrised with Pl / Pr.
+    Returns (A, b, assembly seconds)."""
     from scipy import sparse
     from oracle import fdfd_oracle as O
     t0 = time.perf_counter()
@@ -376,39 +394,68 @@ def cpu_baseline(p, sample_iters: int, iters_full: int, iters_source: str = '') 
     pl = O.precond_pl(p.dxes)
     A = (sparse.diags_array(pl) @ A0 @ sparse.diags_array(1 / pl)).tocsr()
     b = pl * (-1j * p.omega * p.J)
-    t1 = time.perf_counter()
-    scipy.sparse.linalg.qmr(A, b, rtol=1e-30, atol=0.0, maxiter=sample_iters)
-    t2 = time.perf_counter()
-    t_iter = (t2 - t1) / sample_iters
-    t_solve = (t1 - t0) + iters_full * t_iter
+    return A, b, time.perf_counter() - t0
+
+
+def qmr_seconds_per_iteration(A, b, iters: int) -> float:
+    """Wall seconds per scipy QMR iteration over one call of `iters` iterations from zero."""
+    import scipy.sparse.linalg
+    t = time.perf_counter()
+    scipy.sparse.linalg.qmr(A, b, rtol=1e-30, atol=0.0, maxiter=iters)
+    return (time.perf_counter() - t) / iters
+
+
+def extrapolated(t_asm: float, t_iter: float, iters_full: int) -> float:
+    """Seconds of one full reference solve: assembly + iters_full QMR iterations."""
+    return t_asm + iters_full * t_iter
+
+
+def cpu_baseline(p, sample_iters: int, iters_full: int, iters_source: str = '') -> dict:
+    """Oracle port of the reference path timed on the host: assembly + `sample_iters`
+    scipy QMR iterations, extrapolated to `iters_full` iterations per solve."""
+    A, b, t_asm = reference_system(p)
+    t_iter = qmr_seconds_per_iteration(A, b, sample_iters)
+    t_solve = extrapolated(t_asm, t_iter, iters_full)
+    cpu = host_cpu()
     return {'value': float(f'{1.0 / t_solve:.6g}'), 'unit': 'solves/s', 'cores': 1, 'kind': 'port',
-            'sample': f'CSR assembly ({t1 - t0:.1f} s) + {sample_iters} scipy QMR iterations '
-                      f'({t_iter * 1e3:.0f} ms each; scipy\'s CSR product runs on one thread) on the full '
+            'host': cpu,
+            'sample': f'CSR assembly ({t_asm:.1f} s) + {sample_iters} scipy QMR iterations '
+                      f'({t_iter * 1e3:.0f} ms each; scipy\'s CSR product runs on one thread of the '
+                      f'{cpu["nproc"]}-core host) on the full '
                       f'{"x".join(map(str, p.shape))} system, extrapolated to {iters_full} iterations '
                       f'({iters_source or "the GPU complex128 COCG count"})',
             'seconds_per_solve': round(t_solve, 1)}
 
 
 def run_reference(args) -> dict | None:
+    """Each step times `ref_step_iters` QMR iterations of the reference system (assembled
+    once, timed once); the line reports the median step, extrapolated to a full solve."""
     rank = int(os.environ.get('RANK', 0))
     if rank != 0:
         return None
     from meanas_b200 import workloads
     p = workloads.BY_NAME[args.workload]()
-    samples = []
     iters_full, source = REF_ITERS[args.workload]
     if args.ref_iters:
         iters_full, source = args.ref_iters, 'given on the command line'
-    for _ in range(args.warmup + args.steps):
-        samples.append(cpu_baseline(p, args.cpu_sample_iters, iters_full, source))
-    timed = samples[args.warmup:]
-    v = statistics.median(s['value'] for s in timed)
+    A, b, t_asm = reference_system(p)
+    per_iter = [qmr_seconds_per_iteration(A, b, args.ref_step_iters)
+                for _ in range(args.warmup + args.steps)][args.warmup:]
+    t_iter = statistics.median(per_iter)
+    v = float(f'{1.0 / extrapolated(t_asm, t_iter, iters_full):.6g}')
+    cpu = host_cpu()
+    sample = (f'CSR assembly ({t_asm:.1f} s, once) + {args.steps} timed steps of {args.ref_step_iters} '
+              f'scipy QMR iterations each (median {t_iter * 1e3:.0f} ms per iteration, spread '
+              f'{min(per_iter) * 1e3:.0f}-{max(per_iter) * 1e3:.0f} ms; scipy\'s CSR product runs on one '
+              f'thread of the {cpu["nproc"]}-core host) on the full {"x".join(map(str, p.shape))} system, '
+              f'extrapolated to {iters_full} iterations ({source})')
     return {'metric': METRIC, 'value': v, 'unit': 'solves/s', 'n_gpus': args.gpus, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': 1e3 / v, 'higher_is_better': True, 'scaling': 'weak',
             'vs_baseline': None, 'dtype': 'c128', 'data': 'synthetic (seeded)', 'impl': 'reference',
             'config': dict(workload_config(args.workload, p), method='scipy qmr (reference generic() algorithm, CPU)'),
-            'cpu_baseline': {'value': v, 'unit': 'solves/s', 'cores': 1, 'kind': 'port',
-                             'sample': timed[0]['sample']},
+            'cpu_baseline': {'value': v, 'unit': 'solves/s', 'cores': 1, 'kind': 'port', 'host': cpu,
+                             'sample': sample, 'seconds_per_iteration': round(t_iter, 4),
+                             'iterations_extrapolated_to': iters_full},
             'e2e': {'value': v, 'unit': 'solves/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
 
 
@@ -626,7 +673,10 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', choices=['ours', 'reference'], default='ours')
     ap.add_argument('--e2e-steps', type=int, default=2)
-    ap.add_argument('--cpu-sample-iters', type=int, default=4)
+    ap.add_argument('--cpu-sample-iters', type=int, default=12,
+                    help='QMR iterations of the cpu_baseline sample')
+    ap.add_argument('--ref-step-iters', type=int, default=4,
+                    help='QMR iterations per step of the reference arm')
     ap.add_argument('--ref-iters', type=int, default=0,
                     help='QMR iterations per full solve used to extrapolate the reference arm '
                          '(0: the per-workload count in REF_ITERS)')

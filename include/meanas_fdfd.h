@@ -161,7 +161,10 @@ int fdfd_solve(fdfd_plan* plan, const fdfd_solve_opts* opts, const void* J, void
 
 /* FP64 residual norms of a field: out[0] = ||b0 - A0 E||, out[1] = ||Pl (b0 - A0 E)||,
  * out[2] = ||b0||, out[3] = ||Pl b0|| with b0 = -i omega J
- * (the check of meanas/test/test_fdfd.py:14-18).  `ws` >= fdfd_residual_workspace_bytes. */
+ * (the check of meanas/test/test_fdfd.py:14-18).  `ws` >= fdfd_residual_workspace_bytes.
+ * The results pass through the plan's pinned host state, so calls on one plan
+ * (fdfd_residual, fdfd_residual_static, fdfd_solve) must not run at the same time from
+ * different host threads. */
 int fdfd_residual_workspace_bytes(const fdfd_plan* plan, size_t* bytes);
 int fdfd_residual(fdfd_plan* plan, const void* E, const void* J, double out[4], void* ws,
                   size_t ws_bytes, void* stream);
@@ -270,6 +273,11 @@ int fdfd_fdtd_update_e(const fdfd_fdtd_desc* desc, void* E, const void* H, void*
  * with FDFD_ERR_ARG.  The first call on a device looks up that array's device
  * address; make it before any stream capture.  All calls share the array: calls
  * whose work overlaps on the GPU (other streams, other threads) race on it.
+ * Like fdfd_residual, the four results pass through the plan's pinned host state:
+ * calls on one plan (this one, fdfd_residual, fdfd_solve) must not run at the same
+ * time from different host threads, even on one stream.  The looked-up address is
+ * kept for the life of the process: the library must not be used on a device after
+ * that device has been reset (cudaDeviceReset) in the same process.
  * Allocates nothing; same results as fdfd_residual. */
 int fdfd_residual_static(fdfd_plan* plan, const void* E, const void* J, double out[4], void* stream);
 

@@ -237,16 +237,20 @@ static long long max_blocks(const fdfd_plan* P) {
 static std::mutex g_smem_mutex;
 
 template <typename K>
-static void ensure_smem(K kern, size_t bytes) {
-  // only needed above the 48 KB default; remembered per kernel (plans may run on
-  // several host threads at once)
-  static std::vector<const void*> done;
-  if (bytes <= 48 * 1024) return;
-  const void* key = (const void*)kern;
+static int ensure_smem(K kern, size_t bytes) {
+  // Only needed above the 48 KB default.  The attribute belongs to the current
+  // device, so it is remembered per (device, kernel); plans may run on several
+  // host threads at once.
+  static std::vector<std::pair<int, const void*>> done;
+  if (bytes <= 48 * 1024) return 0;
+  int dev = -1;
+  CK(cudaGetDevice(&dev));
+  const std::pair<int, const void*> key(dev, (const void*)kern);
   std::lock_guard<std::mutex> lock(g_smem_mutex);
-  if (std::find(done.begin(), done.end(), key) != done.end()) return;
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (std::find(done.begin(), done.end(), key) != done.end()) return 0;
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
   done.push_back(key);
+  return 0;
 }
 
 template <typename R, class Op>
@@ -257,12 +261,12 @@ static int launch_stencil(fdfd_plan* P, const Geo<R>& g0, int precision, const O
   if (P->flat) {
     using Sh = StencilShape<R, 1, FLAT_TY, true, Op::NB, Op::NO>;
     auto kern = k_stencil<R, 1, FLAT_TY, true, MinBlocks<R>::value, Op>;
-    ensure_smem(kern, Sh::smem_bytes());
+    if (int rc = ensure_smem(kern, Sh::smem_bytes())) return rc;
     kern<<<(unsigned)t.nblocks, dim3(1, FLAT_TY), Sh::smem_bytes(), s>>>(g, op, rb);
   } else {
     using Sh = StencilShape<R, TZ3, TY3, false, Op::NB, Op::NO>;
     auto kern = k_stencil<R, TZ3, TY3, false, MinBlocks<R>::value, Op>;
-    ensure_smem(kern, Sh::smem_bytes());
+    if (int rc = ensure_smem(kern, Sh::smem_bytes())) return rc;
     kern<<<(unsigned)t.nblocks, dim3(TZ3, TY3), Sh::smem_bytes(), s>>>(g, op, rb);
   }
   P->launches++;

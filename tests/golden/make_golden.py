@@ -1,8 +1,8 @@
 """Generate tests/golden/*.npz by running the reference meanas itself.
 
-Run from the repository root, where the reference checkout is mounted:
+Run from the repository root with the path of a reference checkout:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path to the meanas checkout>
 
 The reference is pure Python (numpy/scipy) and imports directly; this script is
 the only place that reads it.  Outputs:
@@ -39,7 +39,9 @@ from pathlib import Path
 
 import numpy
 
-REF = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+if len(sys.argv) < 2:
+    sys.exit('usage: python tests/golden/make_golden.py <path to the meanas checkout> [names...]')
+REF = sys.argv[1]
 sys.path.insert(0, REF)
 sys.path.insert(0, str(Path(__file__).resolve().parents[2]))
 

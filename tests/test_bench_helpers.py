@@ -33,5 +33,12 @@ def test_workload_config_and_peaks():
     assert cfg['shape'] == [48, 48, 48] and cfg['unknowns'] == 3 * 48 ** 3
     peak, kind = bench.peaks()
     assert peak > 1000 and kind in ('measured', 'fallback')
-    assert bench.profile_traffic('cocg_stencil_c128', 'aniso_blocks') > 1e9
-    assert bench.profile_traffic('cocg_stencil_c128', 'dipole_core') is None
+    traffic, source = bench.profile_traffic('cocg_stencil_c128', 'aniso_blocks')
+    assert traffic > 1e9 and source.startswith('profiles/cocg_stencil_c128_aniso160.md')
+    assert bench.profile_traffic('cocg_stencil_c128', 'dipole_core') == (None, None)
+
+
+def test_reference_extrapolation_and_host_description():
+    assert bench.extrapolated(10.0, 0.5, 100) == 60.0
+    cpu = bench.host_cpu()
+    assert cpu['nproc'] >= 1
