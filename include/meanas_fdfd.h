@@ -203,6 +203,32 @@ int fdfd_e2h(fdfd_plan* plan, const void* E, void* H, void* S, int32_t flags, vo
 int fdfd_tfsf_source(fdfd_plan* plan, const void* E, const double* tf_region, void* J, int32_t flags,
                      void* stream);
 
+/* A waveguide cross-section and the half-space of a unidirectional mode source
+ * (the `axis`, `polarity` and `slices` arguments of meanas/fdfd/waveguide_3d.py). */
+typedef struct fdfd_mode_slice {
+  int32_t axis;           /* propagation axis, 0..2                                       */
+  int32_t polarity;       /* +1 or -1                                                     */
+  int32_t lo[3], hi[3];   /* slices as [lo, hi) per axis; hi[axis] = lo[axis] + 1          */
+  int32_t mask_lo, mask_hi; /* planes of the source's half-space mask along the axis       */
+} fdfd_mode_slice;
+
+/* expand_e (meanas/fdfd/waveguide_3d.py:206-257): E_out[c, .., i, ..] = phase[i] *
+ * E_mode[c, .., lo[axis], ..] inside the transverse window, 0 outside; phase =
+ * exp(-i polarity wavenumber r_E) per plane of the axis (complex128[n_axis]).  With
+ * mask_out (float64 [3N], may be NULL) also the half-space mask of compute_source
+ * (1 on planes [mask_lo, mask_hi)).  E_mode, E_out: complex128 [3N] device arrays. */
+int fdfd_mode_expand(fdfd_plan* plan, const void* E_mode, const void* phase, const fdfd_mode_slice* slice,
+                     void* E_out, double* mask_out, void* stream);
+
+/* The unidirectional mode source J = waveguide_3d.compute_source(E_mode, wavenumber,
+ * omega, dxes, axis, polarity, slices, epsilon, mu) (meanas/fdfd/waveguide_3d.py:113-156):
+ * fdfd_mode_expand into E_work / mask_work, then e_boundary_source(mask) @ E_work
+ * (fdfd_tfsf_source with FDFD_SRC_EDGES).  The plan holds omega, dxes, epsilon, mu and
+ * no PEC/PMC.  E_work (complex128 [3N]) and mask_work (float64 [3N]) are caller scratch;
+ * J: complex128 [3N]. */
+int fdfd_mode_source(fdfd_plan* plan, const void* E_mode, const void* phase, const fdfd_mode_slice* slice,
+                     void* E_work, double* mask_work, void* J, void* stream);
+
 /* A general complex128 CSR matrix (device arrays), as scipy.sparse.csr_array holds it:
  * row r's nonzeros are data[indptr[r] .. indptr[r+1]) at columns indices[...]. */
 typedef struct fdfd_csr_desc {

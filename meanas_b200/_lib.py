@@ -90,6 +90,11 @@ class FdtdDesc(C.Structure):  # fdfd_fdtd_desc
                 ('mu', C.c_void_p), ('face', (FdtdFace * 2) * 3)]
 
 
+class ModeSlice(C.Structure):  # fdfd_mode_slice
+    _fields_ = [('axis', C.c_int32), ('polarity', C.c_int32), ('lo', C.c_int32 * 3), ('hi', C.c_int32 * 3),
+                ('mask_lo', C.c_int32), ('mask_hi', C.c_int32)]
+
+
 REAL64, REAL32 = 0, 1
 FDTD_PLAIN, FDTD_CPML = 0, 1
 
@@ -113,6 +118,10 @@ EXPORTS = {
     'fdfd_residual_static': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_void_p]),
     'fdfd_e2h': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     'fdfd_tfsf_source': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    'fdfd_mode_expand': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(ModeSlice), C.c_void_p,
+                                   C.c_void_p, C.c_void_p]),
+    'fdfd_mode_source': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(ModeSlice), C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p]),
     'fdfd_csr_spmv': (C.c_int, [C.POINTER(CsrDesc), C.c_void_p, C.c_void_p, C.c_void_p]),
     'fdfd_csr_solve_workspace_bytes': (C.c_int, [C.POINTER(CsrDesc), C.POINTER(C.c_size_t)]),
     'fdfd_csr_solve': (C.c_int, [C.POINTER(CsrDesc), C.POINTER(SolveOpts), C.c_void_p, C.c_void_p, C.c_void_p,

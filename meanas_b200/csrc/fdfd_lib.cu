@@ -1097,6 +1097,84 @@ extern "C" int fdfd_tfsf_source(fdfd_plan* P, const void* E, const double* tf_re
   return launch_stencil<double>(P, P->g64, 0, op, RedBuf{nullptr, nullptr}, s);
 }
 
+// ------------------------------------------------------------------ waveguide mode source
+// expand_e (meanas/fdfd/waveguide_3d.py:206-257): the mode's cross-section at index s0 of
+// the propagation axis, inside the transverse window [lo, hi), repeated along the whole
+// axis with the per-plane phase table; and the half-space mask compute_source builds
+// (:145-152): 1 on planes [mlo, mhi) of the axis, every component and transverse cell.
+__global__ void k_expand_mode(const cx<double>* __restrict__ Em, const cx<double>* __restrict__ phase,
+                              cx<double>* __restrict__ Eo, double* __restrict__ mask, int X, int Y, int Z,
+                              int axis, int s0, int3 lo, int3 hi, int mlo, int mhi) {
+  const long long N = (long long)X * Y * Z;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 3 * N;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long cell = t % N;
+    const int c = (int)(t / N);
+    const int k = (int)(cell % Z), j = (int)((cell / Z) % Y), i = (int)(cell / ((long long)Y * Z));
+    const int q[3] = {i, j, k};
+    const int l3[3] = {lo.x, lo.y, lo.z}, h3[3] = {hi.x, hi.y, hi.z};
+    bool inside = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+      if (a != axis && (q[a] < l3[a] || q[a] >= h3[a])) inside = false;
+    cx<double> v = mkc<double>(0.0, 0.0);
+    if (inside) {
+      int src[3] = {i, j, k};
+      src[axis] = s0;
+      const cx<double> e = Em[(long long)c * N + ((long long)src[0] * Y + src[1]) * Z + src[2]];
+      v = phase[q[axis]] * e;
+    }
+    Eo[t] = v;
+    if (mask) mask[t] = (q[axis] >= mlo && q[axis] < mhi) ? 1.0 : 0.0;
+  }
+}
+
+static int check_mode_slice(const fdfd_plan* P, const fdfd_mode_slice* m, const char* who) {
+  if (!m) return set_err(FDFD_ERR_ARG, "%s: NULL slice description", who);
+  const int n[3] = {P->X, P->Y, P->Z};
+  if (m->axis < 0 || m->axis > 2) return set_err(FDFD_ERR_ARG, "%s: axis %d", who, m->axis);
+  if (m->polarity != 1 && m->polarity != -1) return set_err(FDFD_ERR_ARG, "%s: polarity %d", who, m->polarity);
+  for (int a = 0; a < 3; ++a)
+    if (m->lo[a] < 0 || m->hi[a] > n[a] || m->lo[a] >= m->hi[a])
+      return set_err(FDFD_ERR_ARG, "%s: slice [%d, %d) of axis %d outside [0, %d)", who, m->lo[a], m->hi[a], a, n[a]);
+  if (m->hi[m->axis] != m->lo[m->axis] + 1)
+    return set_err(FDFD_ERR_ARG, "%s: the slice must select one index along the propagation axis", who);
+  if (m->mask_lo < 0 || m->mask_hi > n[m->axis] || m->mask_lo > m->mask_hi)
+    return set_err(FDFD_ERR_ARG, "%s: mask planes [%d, %d) outside [0, %d)", who, m->mask_lo, m->mask_hi, n[m->axis]);
+  return 0;
+}
+
+static unsigned elementwise_blocks(const fdfd_plan* P, long long n) {
+  const long long need = (n + 255) / 256;
+  return (unsigned)std::max(1LL, std::min(need, 8LL * P->nsm));
+}
+
+extern "C" int fdfd_mode_expand(fdfd_plan* P, const void* E_mode, const void* phase, const fdfd_mode_slice* m,
+                                void* E_out, double* mask_out, void* stream) {
+  if (!P || !E_mode || !phase || !E_out) return set_err(FDFD_ERR_ARG, "fdfd_mode_expand: NULL argument");
+  if (E_mode == E_out) return set_err(FDFD_ERR_ARG, "fdfd_mode_expand: E_out must not alias E_mode");
+  TRY(check_mode_slice(P, m, "fdfd_mode_expand"));
+  k_expand_mode<<<elementwise_blocks(P, 3 * P->N), 256, 0, (cudaStream_t)stream>>>(
+      (const cx<double>*)E_mode, (const cx<double>*)phase, (cx<double>*)E_out, mask_out, P->X, P->Y, P->Z,
+      m->axis, m->lo[m->axis], make_int3(m->lo[0], m->lo[1], m->lo[2]), make_int3(m->hi[0], m->hi[1], m->hi[2]),
+      m->mask_lo, m->mask_hi);
+  P->launches = 1;
+  CKL();
+  return 0;
+}
+
+extern "C" int fdfd_mode_source(fdfd_plan* P, const void* E_mode, const void* phase, const fdfd_mode_slice* m,
+                                void* E_work, double* mask_work, void* J, void* stream) {
+  if (!P || !E_mode || !phase || !E_work || !mask_work || !J)
+    return set_err(FDFD_ERR_ARG, "fdfd_mode_source: NULL argument");
+  if (J == E_work || J == E_mode || E_work == E_mode)
+    return set_err(FDFD_ERR_ARG, "fdfd_mode_source: J, E_work and E_mode must be distinct");
+  TRY(fdfd_mode_expand(P, E_mode, phase, m, E_work, mask_work, stream));
+  TRY(fdfd_tfsf_source(P, E_work, mask_work, J, FDFD_SRC_EDGES, stream));
+  P->launches += 1;
+  return 0;
+}
+
 // ------------------------------------------------------------------ CSR solves
 static int csr_view(const fdfd_csr_desc* d, CsrView* v, const char* who) {
   if (!d) return set_err(FDFD_ERR_ARG, "%s: NULL matrix", who);

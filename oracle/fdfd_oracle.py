@@ -37,6 +37,10 @@ What each function restates:
   (``meanas/fdfd/operators.py:366-393``) and, with ``edges``, the edge mask of
   ``e_boundary_source`` (``:396-450``; mirrored or periodic one-cell shifts,
   ``meanas/fdmath/operators.py:55-98``).
+* ``expand_e`` / ``mode_source``  the unidirectional waveguide-mode source:
+  ``meanas/fdfd/waveguide_3d.py:206-257`` (the source-plane cross-section repeated along the
+  axis with the phase ``exp(-i polarity k r)``) and ``:113-156`` (the boundary source of that
+  field on the half-space mask from the source plane onward).
 * ``fdtd_plain_step`` / ``CpmlUpdates``  the FDTD Yee updates: ``maxwell_h`` /
   ``maxwell_e`` (``meanas/fdtd/base.py:13-125``) and ``updates_with_cpml``
   (``meanas/fdtd/pml.py:115-230``, which divides its forward differences by the H-grid
@@ -162,6 +166,39 @@ def tfsf_source(omega, dxes, epsilon, E, tf_region, mu=None, *, edges=False, per
         shape = _shape_of(dxes)
         j = j * _edge_mask(q.reshape(3, *shape), periodic).ravel()
     return j
+
+
+def expand_e(E, wavenumber, dxes, axis: int, polarity: int, slices) -> NDArray:
+    """(3,X,Y,Z) field: the cross-section of ``E`` at ``slices`` repeated along ``axis``
+    with phase ``exp(-i polarity wavenumber r)`` (``meanas/fdfd/waveguide_3d.py:232-257``)."""
+    E = numpy.asarray(E, dtype=complex)
+    slices = tuple(slices)
+    pos = numpy.cumsum(numpy.real(numpy.asarray(dxes[0][axis])))
+    dist = pos - pos[slices[axis]]
+    ph = numpy.exp(polarity * -1j * wavenumber * dist)
+    bshape = [1, 1, 1, 1]
+    bshape[axis + 1] = -1
+    out = numpy.zeros_like(E)
+    dst = [slice(None), *slices]
+    dst[axis + 1] = slice(None)
+    out[tuple(dst)] = ph.reshape(bshape) * E[(slice(None), *slices)]
+    return out
+
+
+def mode_source(E, wavenumber, omega, dxes, axis: int, polarity: int, slices, epsilon, mu=None) -> NDArray:
+    """(3,X,Y,Z) current of the unidirectional mode source (``meanas/fdfd/waveguide_3d.py:113-156``):
+    the boundary source (``tfsf_source(..., edges=True)``) of ``expand_e`` on the half-space
+    from ``slices[axis].start`` onward (``polarity > 0``) or up to ``slices[axis].stop``."""
+    Ee = expand_e(E, wavenumber, dxes, axis, polarity, slices)
+    sl = tuple(slices)[axis]
+    q = numpy.zeros(Ee.shape)
+    half = [slice(None)] * 4
+    half[axis + 1] = slice(sl.start, None) if polarity > 0 else slice(None, sl.stop)
+    q[tuple(half)] = 1.0
+    eps = numpy.asarray(epsilon).ravel()
+    mu = None if mu is None else numpy.asarray(mu).ravel()
+    J = tfsf_source(omega, dxes, eps, Ee.ravel(), q.ravel(), mu, edges=True)
+    return J.reshape(Ee.shape)
 
 
 def fdtd_plain_step(e: NDArray, h: NDArray, epsilon: NDArray, dt: float, dxes) -> None:

@@ -30,6 +30,16 @@ the only place that reads it.  Outputs:
                     CPML parameter tables.
 * ``dipole48.npz``  reference ``generic()`` on the 48^3 dipole-in-core problem
                     (rtol 1e-8, scipy QMR): field stored as complex64.
+* ``modesrc.npz``   ``waveguide_3d.expand_e`` and ``waveguide_3d.compute_source`` with their
+                    inputs: the mode fields of ``meanas/test/test_fdfd_pml.py`` on its 1D
+                    grids, and random cross-section fields on 3D grids (PML, non-uniform
+                    widths, mu, partial transverse windows, complex wavenumbers, every axis
+                    and both polarities).
+* ``grad96.npz``    the adjoint gradient of the 96x96x64 design problem from the reference's
+                    own solves: ``generic()`` for E, ``generic(adjoint=True)`` with
+                    ``-i omega J_adj = 2 E`` on the monitor plane, ``dL/deps =
+                    Re(omega^2 conj(E_adj) E)`` over the 40x40x8 design region (not part of
+                    the default set: two QMR solves of 1.77M unknowns take a while).
 """
 from __future__ import annotations
 
@@ -445,8 +455,131 @@ def gen_dipole48() -> None:
     print('dipole48', it[0], t1 - t0, res)
 
 
+def gen_modesrc() -> None:
+    out = {}
+    n = 0
+
+    def store(shape, dxes, eps, mu, E, k, om, axis, pol, sl):
+        nonlocal n
+        p = f'c{n}_'
+        Ee = waveguide_3d.expand_e(E=E, wavenumber=k, dxes=dxes, axis=axis, polarity=pol, slices=sl)
+        J = waveguide_3d.compute_source(E=E, wavenumber=k, omega=om, dxes=dxes, axis=axis, polarity=pol,
+                                        slices=sl, epsilon=eps, mu=mu)
+        out[p + 'shape'] = numpy.array(shape)
+        out[p + 'omega'] = numpy.array(complex(om))
+        out[p + 'k'] = numpy.array(complex(k))
+        out[p + 'axis'] = numpy.array(axis)
+        out[p + 'polarity'] = numpy.array(pol)
+        out[p + 'slices'] = numpy.array([[s_.start if s_.start is not None else -(10 ** 9),
+                                          s_.stop if s_.stop is not None else 10 ** 9] for s_ in sl])
+        pack_dxes(p, dxes, out)
+        out[p + 'eps'] = eps
+        if mu is not None:
+            out[p + 'mu'] = mu
+        out[p + 'E'] = E
+        out[p + 'E_expanded'] = numpy.asarray(Ee)
+        out[p + 'J'] = numpy.asarray(J)
+        n += 1
+
+    # meanas/test/test_fdfd_pml.py: the hand-built mode on 1D grids (fixtures there)
+    om = 1 / 1500
+    for shape in [(30, 1, 1), (1, 30, 1), (1, 1, 30)]:
+        for pol in (+1, -1):
+            for fg in (1.0, 2.5):
+                dx = 1.0 if fg == 1.0 else 1.5
+                sh3 = (3, *shape)
+                eps = numpy.full(sh3, fg)
+                dxes = [[numpy.full(s_, dx) for s_ in shape] for _ in range(2)]
+                dim = int(numpy.where(numpy.array(shape) > 1)[0][0])
+                for p_ in (-1, 1):
+                    dxes = scpml.stretch_with_scpml(dxes, axis=dim, polarity=p_, omega=om,
+                                                    epsilon_effective=fg, thickness=10)
+                other = [0, 1, 2]
+                other.remove(dim)
+                dx_prop = (dxes[0][dim][shape[dim] // 2] + dxes[1][dim][shape[dim] // 2]) / 2
+                cm = numpy.zeros(sh3, dtype=bool)
+                cm[other, shape[0] // 2, shape[1] // 2, shape[2] // 2] = True
+                k = om * numpy.sqrt(eps[cm].mean())
+                kc = 2 / dx_prop * numpy.arcsin(k * dx_prop / 2)
+                e = numpy.zeros_like(eps, dtype=complex)
+                e[cm] = 1 / numpy.linalg.norm(cm[:])
+                sl = [slice(None)] * 3
+                sl[dim] = slice(shape[dim] // 2, shape[dim] // 2 + 1)
+                store(shape, [list(d) for d in dxes], eps, None, e, kc, om, dim, pol, sl)
+
+    # 3D grids: random cross-section fields in partial windows, PML, mu, complex wavenumbers
+    rng = numpy.random.default_rng(77)
+    for shape, axis, pol, th, use_mu in [((14, 11, 9), 0, 1, 3, False), ((14, 11, 9), 0, -1, 3, True),
+                                         ((9, 16, 10), 1, 1, 2, True), ((9, 16, 10), 1, -1, 0, False),
+                                         ((10, 9, 17), 2, 1, 3, True), ((10, 9, 17), 2, -1, 3, False),
+                                         ((12, 13, 1), 0, 1, 3, False), ((1, 12, 13), 2, -1, 2, True)]:
+        om3 = 2 * numpy.pi / rng.uniform(6, 10)
+        dxes = [[rng.uniform(0.8, 1.2, s_) for s_ in shape] for _ in range(2)]
+        for ax in range(3):
+            if th and shape[ax] > 2 * th + 1:
+                for p_ in (-1, 1):
+                    dxes = scpml.stretch_with_scpml(dxes, axis=ax, polarity=p_, omega=om3, thickness=th)
+        sh3 = (3, *shape)
+        eps = rng.uniform(1, 12, sh3)
+        mu = rng.uniform(1, 1.5, sh3) if use_mu else None
+        s0 = int(rng.integers(2, shape[axis] - 2)) if shape[axis] > 4 else 0
+        sl = []
+        for a, n_a in enumerate(shape):
+            if a == axis:
+                sl.append(slice(s0, s0 + 1))
+            elif n_a > 4:
+                lo = int(rng.integers(0, n_a // 3))
+                sl.append(slice(lo, n_a - int(rng.integers(0, n_a // 3))))
+            else:
+                sl.append(slice(None))
+        E = numpy.zeros(sh3, dtype=complex)
+        E[(slice(None), *sl)] = rng.standard_normal((3, *E[(0, *sl)].shape)) + \
+            1j * rng.standard_normal((3, *E[(0, *sl)].shape))
+        k = om3 * rng.uniform(1.2, 3.0) * (1 - 0.01j)
+        store(shape, dxes, eps, mu, E, k, om3, axis, pol, sl)
+    out['n'] = numpy.array(n)
+    numpy.savez_compressed(OUT / 'modesrc.npz', **out)
+
+
+def gen_grad96() -> None:
+    from meanas_b200 import workloads
+    p = workloads.adjoint_design()
+    its = []
+
+    def qmr_counting(A, b, **kw):
+        it = [0]
+
+        def cb(_):
+            it[0] += 1
+        x = scipy.sparse.linalg.qmr(A, b, callback=cb, **kw)[0]
+        its.append(it[0])
+        return x
+    opts = dict(rtol=1e-10, atol=0)
+    t0 = time.perf_counter()
+    E = solvers.generic(p.omega, p.dxes, p.J, p.epsilon, matrix_solver=qmr_counting,
+                        matrix_solver_opts=opts)
+    mon = p.extra['monitor']
+    G = 2 * E * mon                     # dL/dE* convention of torch: L = sum |E|^2 on the plane
+    J_adj = G / (-1j * p.omega)
+    E_adj = solvers.generic(p.omega, p.dxes, J_adj, p.epsilon, adjoint=True,
+                            matrix_solver=qmr_counting, matrix_solver_opts=opts)
+    t1 = time.perf_counter()
+    grad = numpy.real(p.omega ** 2 * numpy.conj(E_adj) * E).reshape(3, *p.shape)
+    dsl = p.extra['design_slices']
+    A0 = operators.e_full(p.omega, p.dxes, p.epsilon).tocsr()
+    b0 = -1j * p.omega * p.J
+    res = numpy.linalg.norm(A0 @ E - b0) / numpy.linalg.norm(b0)
+    ba = -1j * p.omega * J_adj
+    res_adj = numpy.linalg.norm(A0.conj().T @ E_adj - ba) / numpy.linalg.norm(ba)
+    numpy.savez_compressed(OUT / 'grad96.npz', grad_design=grad[(slice(None), *dsl)],
+                           eps_design=p.epsilon.reshape(3, *p.shape)[(slice(None), *dsl)],
+                           loss=float(numpy.sum(numpy.abs(E[mon]) ** 2)), qmr_iterations=numpy.array(its),
+                           seconds=t1 - t0, residual=res, residual_adjoint=res_adj, rtol=opts['rtol'])
+    print('grad96', its, t1 - t0, res, res_adj)
+
+
 if __name__ == '__main__':
-    which = sys.argv[2:] or ['scpml', 'operator', 'e2h', 'sources', 'fdtd', 'solve', 'dipole48']
+    which = sys.argv[2:] or ['scpml', 'operator', 'e2h', 'sources', 'fdtd', 'solve', 'dipole48', 'modesrc']
     for w in which:
         t = time.perf_counter()
         globals()[f'gen_{w}']()

@@ -42,10 +42,11 @@ def test_struct_layouts_match_header(tmp_path: Path):
 #include <stddef.h>
 #include "{HEADER}"
 int main(void) {{
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(fdfd_grid_desc), sizeof(fdfd_solve_opts),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(fdfd_grid_desc), sizeof(fdfd_solve_opts),
          sizeof(fdfd_solve_info), offsetof(fdfd_grid_desc, epsilon), offsetof(fdfd_solve_opts, history),
          offsetof(fdfd_solve_info, residual), sizeof(fdfd_csr_desc), offsetof(fdfd_csr_desc, data),
-         sizeof(fdfd_fdtd_face), sizeof(fdfd_fdtd_desc), offsetof(fdfd_fdtd_desc, face));
+         sizeof(fdfd_fdtd_face), sizeof(fdfd_fdtd_desc), offsetof(fdfd_fdtd_desc, face),
+         sizeof(fdfd_mode_slice), offsetof(fdfd_mode_slice, mask_lo));
   return 0;
 }}
 ''')
@@ -55,7 +56,8 @@ int main(void) {{
     want = [C.sizeof(_lib.GridDesc), C.sizeof(_lib.SolveOpts), C.sizeof(_lib.SolveInfo),
             _lib.GridDesc.epsilon.offset, _lib.SolveOpts.history.offset, _lib.SolveInfo.residual.offset,
             C.sizeof(_lib.CsrDesc), _lib.CsrDesc.data.offset,
-            C.sizeof(_lib.FdtdFace), C.sizeof(_lib.FdtdDesc), _lib.FdtdDesc.face.offset]
+            C.sizeof(_lib.FdtdFace), C.sizeof(_lib.FdtdDesc), _lib.FdtdDesc.face.offset,
+            C.sizeof(_lib.ModeSlice), _lib.ModeSlice.mask_lo.offset]
     assert got == want
 
 

@@ -157,3 +157,22 @@ def test_pml_fixture_assertions_hold_for_reference_solutions():
             tgt, rev = rev, tgt
         numpy.testing.assert_allclose(rev, 0, atol=1e-12)
         numpy.testing.assert_allclose(tgt, 1, rtol=3e-6)
+
+
+MODESRC = golden_cases('modesrc')
+
+
+def _slices(c):
+    big = 10 ** 9
+    return [slice(None if lo == -big else int(lo), None if hi == big else int(hi)) for lo, hi in c['slices']]
+
+
+@pytest.mark.parametrize('c', MODESRC, ids=lambda c: f"mode{c['index']}-{tuple(int(s) for s in c['shape'])}")
+def test_oracle_mode_source_matches_reference(c):
+    args = (c['E'], complex(c['k']))
+    axis, pol = int(c['axis']), int(c['polarity'])
+    Ee = O.expand_e(*args, c['dxes'], axis, pol, _slices(c))
+    assert numpy.linalg.norm(Ee - c['E_expanded']) <= 1e-14 * numpy.linalg.norm(c['E_expanded'])
+    J = O.mode_source(*args, complex(c['omega']), c['dxes'], axis, pol, _slices(c), c['eps'], c.get('mu'))
+    assert numpy.linalg.norm(J - c['J']) <= 1e-13 * numpy.linalg.norm(c['J'])
+    assert numpy.array_equal(J == 0, c['J'] == 0)
