@@ -281,7 +281,11 @@ def run_ours(args) -> dict | None:
         assert E.shape == (p.n_unknowns,)
         table_bytes = sum(16 * 2 * numpy.size(d) for g in p.dxes for d in g)
         opt_bytes = sum(8 * a.size for a in (p.mu, p.pec, p.pmc) if a is not None)
+        from meanas_b200.solvers import last_solve_info
+        e2e_info = last_solve_info()
         e2e = dict(value=world * args.e2e_steps / el, unit='solves/s', method=prec,
+                   iterations=e2e_info.iterations, residual=e2e_info.residual,
+                   tiling='a fresh plan per call, as generic() builds it, with the x-chunk tuned for this grid size',
                    h2d_bytes_per_step=int(Jh.numel() * 16 + epsh.numel() * 8 + table_bytes + opt_bytes),
                    d2h_bytes_per_step=int(p.n_unknowns * 16))
 
@@ -333,8 +337,11 @@ def run_ours(args) -> dict | None:
         'e2e': e2e,
     }
     if world == 1 and args.cpu_sample_iters > 0:
-        res['cpu_baseline'] = cpu_baseline(p, args.cpu_sample_iters,
-                                           out['cocg']['iterations'] if 'cocg' in out else b['iterations'])
+        cb = cpu_baseline(p, args.cpu_sample_iters, out['cocg']['iterations'] if 'cocg' in out else b['iterations'],
+                          fields=fields)
+        # the timed fields checked on the host with the reference's CSR operator
+        res['oracle_residual'] = cb.pop('oracle_residual', None)
+        res['cpu_baseline'] = cb
     return res
 
 
@@ -383,18 +390,39 @@ def host_cpu() -> dict:
     return {'nproc': os.cpu_count(), 'model': model}
 
 
-def reference_system(p):
-    """The system the reference's generic() hands to scipy's QMR, built by the oracle port:
-    CSR A0 (mu, PEC and PMC enter as in the reference's e_full), symmetrised with Pl / Pr.
-    Returns (A, b, assembly seconds)."""
-    from scipy import sparse
+def reference_operator(p):
+    """CSR A0 as the reference's e_full assembles it (mu, PEC and PMC included), built by the
+    oracle port.  Returns (A0, assembly seconds)."""
     from oracle import fdfd_oracle as O
     t0 = time.perf_counter()
     A0 = O.e_full_csr(p.omega, p.dxes, p.epsilon, p.mu, p.pec, p.pmc)
+    return A0, time.perf_counter() - t0
+
+
+def reference_system(p, A0=None, t_a0: float = 0.0):
+    """The system the reference's generic() hands to scipy's QMR: A0 symmetrised with
+    Pl / Pr (oracle port).  Returns (A, b, assembly seconds)."""
+    from scipy import sparse
+    from oracle import fdfd_oracle as O
+    if A0 is None:
+        A0, t_a0 = reference_operator(p)
+    t0 = time.perf_counter()
     pl = O.precond_pl(p.dxes)
     A = (sparse.diags_array(pl) @ A0 @ sparse.diags_array(1 / pl)).tocsr()
     b = pl * (-1j * p.omega * p.J)
-    return A, b, time.perf_counter() - t0
+    return A, b, t_a0 + time.perf_counter() - t0
+
+
+def oracle_residuals(p, A0, fields: dict) -> dict:
+    """||b0 - A0 E|| / ||b0|| of each timed GPU field with the host CSR operator of the
+    reference's e_full (the test of meanas/test/test_fdfd.py:14-18), in FP64 on the CPU."""
+    b0 = -1j * p.omega * p.J
+    nb = numpy.linalg.norm(b0)
+    out = {}
+    for m, E in fields.items():
+        e = E.detach().cpu().numpy()
+        out['fp64' if m == 'cocg' else m] = float(numpy.linalg.norm(A0 @ e - b0) / nb)
+    return out
 
 
 def qmr_seconds_per_iteration(A, b, iters: int) -> float:
@@ -410,21 +438,29 @@ def extrapolated(t_asm: float, t_iter: float, iters_full: int) -> float:
     return t_asm + iters_full * t_iter
 
 
-def cpu_baseline(p, sample_iters: int, iters_full: int, iters_source: str = '') -> dict:
+def cpu_baseline(p, sample_iters: int, iters_full: int, iters_source: str = '', fields: dict | None = None) -> dict:
     """Oracle port of the reference path timed on the host: assembly + `sample_iters`
-    scipy QMR iterations, extrapolated to `iters_full` iterations per solve."""
-    A, b, t_asm = reference_system(p)
+    scipy QMR iterations, extrapolated to `iters_full` iterations per solve.  The assembled
+    CSR operator also checks the timed GPU fields (`fields`): their true residuals go in
+    the result's 'oracle_residual'."""
+    A0, t_a0 = reference_operator(p)
+    checked = oracle_residuals(p, A0, fields) if fields else None
+    A, b, t_asm = reference_system(p, A0, t_a0)
+    del A0
     t_iter = qmr_seconds_per_iteration(A, b, sample_iters)
     t_solve = extrapolated(t_asm, t_iter, iters_full)
     cpu = host_cpu()
-    return {'value': float(f'{1.0 / t_solve:.6g}'), 'unit': 'solves/s', 'cores': 1, 'kind': 'port',
-            'host': cpu,
-            'sample': f'CSR assembly ({t_asm:.1f} s) + {sample_iters} scipy QMR iterations '
-                      f'({t_iter * 1e3:.0f} ms each; scipy\'s CSR product runs on one thread of the '
-                      f'{cpu["nproc"]}-core host) on the full '
-                      f'{"x".join(map(str, p.shape))} system, extrapolated to {iters_full} iterations '
-                      f'({iters_source or "the GPU complex128 COCG count"})',
-            'seconds_per_solve': round(t_solve, 1)}
+    out = {'value': float(f'{1.0 / t_solve:.6g}'), 'unit': 'solves/s', 'cores': 1, 'kind': 'port',
+           'host': cpu,
+           'sample': f'CSR assembly ({t_asm:.1f} s) + {sample_iters} scipy QMR iterations '
+                     f'({t_iter * 1e3:.0f} ms each; scipy\'s CSR product runs on one thread of the '
+                     f'{cpu["nproc"]}-core host) on the full '
+                     f'{"x".join(map(str, p.shape))} system, extrapolated to {iters_full} iterations '
+                     f'({iters_source or "the GPU complex128 COCG count"})',
+           'seconds_per_solve': round(t_solve, 1)}
+    if checked is not None:
+        out['oracle_residual'] = checked
+    return out
 
 
 def run_reference(args) -> dict | None:
@@ -569,8 +605,16 @@ def kernel_mode(args) -> None:
 
 def gradient_check(args) -> dict:
     """dL/d(eps) on the 96x96x64 adjoint problem (L = sum |E|^2 over the plane x=76) by
-    torch.autograd (one forward + one adjoint GPU solve) against central finite differences
-    (h = 1e-4, FP64 solves to relative residual 1e-12) on `fd_cells` random design cells."""
+    torch.autograd (one forward + one adjoint GPU solve), checked two ways:
+
+    * against the reference's own adjoint gradient (tests/golden/grad96.npz: the reference
+      generic() forward solve and generic(adjoint=True) solve, scipy QMR to rtol 1e-10,
+      formed over the whole 40x40x8 design region);
+    * against central finite differences of GPU FP64 solves (rtol 1e-12) on `fd_cells`
+      random design cells, Richardson-extrapolated from steps h and h/2
+      ((4 D(h/2) - D(h)) / 3, truncation O(h^4)) so that a step large enough to keep the
+      solves' residual noise (about rtol L / (2 h |g|)) small can be used.
+    """
     import torch
     from meanas_b200 import workloads
     from meanas_b200.autograd import fdfd_solve
@@ -591,36 +635,62 @@ def gradient_check(args) -> dict:
     t_grad = time.perf_counter() - t0
     g = eps.grad.cpu().numpy()
     n = p.n_cells
+    dsl = p.extra['design_slices']
+    g_design = g.reshape(3, *p.shape)[(slice(None), *dsl)]
+    out = {'metric': 'adjoint gradient dL/deps vs the reference adjoint gradient and finite differences',
+           'workload': 'adjoint_design 96x96x64, 10-cell SC-PML, omega=2pi/26, 40x40x8 design, L=sum|E|^2 at x=76',
+           'gradient_seconds': round(t_grad, 3), 'loss': L.item(),
+           'grad_norm_design': float(numpy.linalg.norm(g_design))}
+    ref_file = ROOT / 'tests' / 'golden' / 'grad96.npz'
+    if ref_file.exists():
+        z = numpy.load(ref_file)
+        if numpy.array_equal(z['eps_design'], p.epsilon.reshape(3, *p.shape)[(slice(None), *dsl)]):
+            gr = z['grad_design']
+            cell_gr, cell_g = gr.sum(axis=0), g_design.sum(axis=0)   # d/d(eps of a cell, all 3 components)
+            sig = numpy.abs(cell_gr) >= 1e-3 * numpy.abs(cell_gr).max()
+            out['vs_reference_adjoint'] = {
+                'normwise_rel_err': float(numpy.linalg.norm(g_design - gr) / numpy.linalg.norm(gr)),
+                'max_rel_err_significant_cells': float(numpy.max(numpy.abs(cell_g - cell_gr)[sig] /
+                                                                 numpy.abs(cell_gr)[sig])),
+                'significant_cells': int(sig.sum()), 'cells': int(sig.size),
+                'reference_loss': float(z['loss']), 'loss_rel_err': abs(L.item() - float(z['loss'])) / float(z['loss']),
+                'reference': 'reference generic() + generic(adjoint=True), scipy QMR rtol 1e-10 '
+                             f'(iterations {z["qmr_iterations"].tolist()}, residuals {float(z["residual"]):.1e} / '
+                             f'{float(z["residual_adjoint"]):.1e})'}
+        else:
+            out['vs_reference_adjoint'] = {'error': 'grad96.npz was made for another design region'}
     cells = numpy.flatnonzero(p.extra['design_mask'].ravel())
     rng = numpy.random.default_rng(0)
-    h = 1e-4
-    errs, fds, ads = [], [], []
+    h = args.fd_h
+    errs, errs_plain, fds, ads = [], [], [], []
+
+    def central(idx, step):
+        ep = eps.detach().clone()
+        em = eps.detach().clone()
+        ep[idx] += step
+        em[idx] -= step
+        return (loss(ep) - loss(em)).item() / (2 * step)
     with torch.no_grad():
         for cell in rng.choice(cells, args.fd_cells, replace=False):
             idx = [cell, n + cell, 2 * n + cell]
-            ep = eps.detach().clone()
-            em = eps.detach().clone()
-            ep[idx] += h
-            em[idx] -= h
-            fd = (loss(ep) - loss(em)).item() / (2 * h)
+            d1, d2 = central(idx, h), central(idx, h / 2)
+            fd = (4 * d2 - d1) / 3
             ad = float(g[idx].sum())
             errs.append(abs(fd - ad) / max(abs(fd), 1e-300))
+            errs_plain.append(abs(d2 - ad) / max(abs(d2), 1e-300))
             fds.append(fd)
             ads.append(ad)
     fds, ads = numpy.array(fds), numpy.array(ads)
-    # Per-cell relative errors are dominated by finite-difference noise where the gradient is
-    # tiny (the solves' 1e-12 residual divided by 2h); the normwise error over the sampled
-    # cells and the per-cell error on cells carrying >= 1e-3 of the largest |dL/deps| are not.
     big = numpy.abs(fds) >= 1e-3 * numpy.abs(fds).max()
-    design_g = g[numpy.tile(p.extra['design_mask'].ravel(), 3)]
-    return {'metric': 'adjoint gradient dL/deps vs central finite differences', 'workload':
-            'adjoint_design 96x96x64, 10-cell SC-PML, omega=2pi/26, 40x40x8 design, L=sum|E|^2 at x=76',
-            'fd_cells': args.fd_cells, 'h': h, 'solve_rtol': 1e-12, 'max_rel_err': max(errs),
-            'median_rel_err': float(numpy.median(errs)),
-            'normwise_rel_err': float(numpy.linalg.norm(fds - ads) / numpy.linalg.norm(fds)),
-            'max_rel_err_significant_cells': float(numpy.max(numpy.array(errs)[big])),
-            'significant_cells': int(big.sum()), 'gradient_seconds': round(t_grad, 3),
-            'loss': L.item(), 'grad_norm_design': float(numpy.linalg.norm(design_g))}
+    out.update({'fd_cells': args.fd_cells, 'h': h, 'fd': 'Richardson (4 D(h/2) - D(h)) / 3 of central differences',
+                'solve_rtol': 1e-12, 'max_rel_err': max(errs), 'median_rel_err': float(numpy.median(errs)),
+                'normwise_rel_err': float(numpy.linalg.norm(fds - ads) / numpy.linalg.norm(fds)),
+                'max_rel_err_significant_cells': float(numpy.max(numpy.array(errs)[big])),
+                'significant_cells': int(big.sum()),
+                'plain_central_h_over_2': {'max_rel_err_significant_cells':
+                                           float(numpy.max(numpy.array(errs_plain)[big])),
+                                           'median_rel_err': float(numpy.median(errs_plain))}})
+    return out
 
 
 def serving_run(args) -> dict:
@@ -700,6 +770,7 @@ def main():
     ap.add_argument('--serving-maxiter', type=int, default=50000, help='serving: Krylov iteration cap per request')
     ap.add_argument('--serving-precision', default='mixed', choices=['mixed', 'fp64'])
     ap.add_argument('--fd-cells', type=int, default=64)
+    ap.add_argument('--fd-h', type=float, default=1e-2, help='finite-difference step (and h/2)')
     args = ap.parse_args()
     if args.kernel_iters > 0:
         return kernel_mode(args)

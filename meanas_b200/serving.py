@@ -28,7 +28,13 @@ from typing import Any
 import numpy
 import torch
 
+from . import operators
 from .operators import GridOperator, SolveInfo
+
+# one autotuning run per (device, grid size, precision) at a time; later slots of that
+# size take its result, so every slot of a size has the same tiling
+_TUNE_LOCKS: dict[tuple, threading.Lock] = collections.defaultdict(threading.Lock)
+_TUNE_GUARD = threading.Lock()
 
 
 @dataclasses.dataclass
@@ -71,19 +77,36 @@ def slot_bytes(shape: tuple[int, int, int], precision: str) -> int:
 
 
 class _Slot:
-    def __init__(self, shape, req: Request, device: torch.device, precision: str, xchunk: int | None):
+    def __init__(self, shape, req: Request, device: torch.device, precision: str, xchunk: int | None,
+                 autotune: bool = True):
         self.shape = shape
         self.precision = precision
         self.stream = torch.cuda.Stream(device=device)
+        prec = 'c64' if precision == 'mixed' else 'c128'
         with torch.cuda.device(device), torch.cuda.stream(self.stream):
             self.op = GridOperator(req.omega, req.dxes, req.epsilon, device=device, fp32=(precision == 'mixed'))
             if xchunk:
-                self.op.set_xchunk('c64' if precision == 'mixed' else 'c128', xchunk)
+                self.op.set_xchunk(prec, xchunk)
+                self.xchunk = xchunk
+            elif autotune:
+                # the first slot of a size times the x-chunk candidates on its own stream
+                key = (self.op.device.index, tuple(shape), prec)
+                with _TUNE_GUARD:
+                    lock = _TUNE_LOCKS[key]
+                with lock:
+                    tuned = operators._TUNED.get(key)
+                    if tuned is None:
+                        self.op.autotune(methods=('mixed' if precision == 'mixed' else 'cocg',))
+                    else:
+                        self.op.set_xchunk(prec, tuned)
+                    self.xchunk = operators._TUNED.get(key)
             self.J = torch.empty(self.op.n, dtype=torch.complex128, device=device)
             self.E = torch.empty(self.op.n, dtype=torch.complex128, device=device)
             self.E_host = torch.empty(self.op.n, dtype=torch.complex128).pin_memory()
         self.fresh = True
         self.bytes = slot_bytes(shape, precision)
+
+    xchunk: int | None = None
 
     def close(self):
         self.op.close()
@@ -95,13 +118,15 @@ class FDFDServer:
     ``max_active``: solves in flight at once.  ``hbm_budget``: bytes of device memory
     the slots may hold (default: 80 % of free memory at start-up).  ``precision``:
     ``'mixed'`` (complex64 BiCGSTAB + complex128 refinement) or ``'fp64'`` (COCG).
-    ``rtol``: true FP64 residual target.  ``xchunk``: optional fixed x planes per CTA
-    (otherwise the library's default for each size).
+    ``rtol``: true FP64 residual target.  ``xchunk``: optional fixed x planes per CTA;
+    otherwise (``autotune=True``) the first slot of each grid size times the candidates
+    (``GridOperator.autotune``) and every later slot of that size reuses the choice, or
+    (``autotune=False``) the library's default.
     """
 
     def __init__(self, device: Any | None = None, *, max_active: int = 8, hbm_budget: int | None = None,
                  precision: str = 'mixed', rtol: float = 1e-8, maxiter: int | None = 200000,
-                 xchunk: int | None = None):
+                 xchunk: int | None = None, autotune: bool = True):
         self.device = torch.device(device) if device is not None else torch.device('cuda', 0)
         self._slot_factory = _Slot
         if hbm_budget is None:
@@ -112,6 +137,7 @@ class FDFDServer:
         self.rtol = rtol
         self.maxiter = maxiter
         self.xchunk = xchunk
+        self.autotune = autotune
         self._method = 'mixed' if precision == 'mixed' else 'cocg'
         self._cv = threading.Condition()
         self._waiting: collections.deque[tuple[Request, concurrent.futures.Future]] = collections.deque()
@@ -200,7 +226,9 @@ class FDFDServer:
             req, fut, slot = item
             try:
                 if slot is None:
-                    slot = self._slot_factory(req.shape, req, self.device, self.precision, self.xchunk)
+                    slot = self._slot_factory(req.shape, req, self.device, self.precision, self.xchunk,
+                                              self.autotune)
+                    self.stats['slot_tuned'] += int(getattr(slot, 'xchunk', None) is not None)
                 fut.set_result(self._run(slot, req))
             except BaseException as exc:  # the error goes to the caller
                 fut.set_exception(exc)

@@ -79,6 +79,25 @@ def test_dipole48_matches_reference_field(cuda):
         assert numpy.linalg.norm(E - ref) <= 1e-5 * numpy.linalg.norm(ref), method
 
 
+@pytest.mark.parametrize('method', ['cocg', 'mixed'])
+def test_reported_residual_agrees_with_host_oracle_at_96(cuda, method):
+    """The solver's FP64 true residual, on the 96x96x64 design problem (1.77M unknowns),
+    equals ||b0 - A0 E|| / ||b0|| formed on the host with the reference's CSR operator
+    (oracle port of meanas/fdfd/operators.py:40-96), and both meet rtol."""
+    from meanas_b200 import workloads
+    from meanas_b200.operators import GridOperator
+    from oracle import fdfd_oracle as O
+    p = workloads.adjoint_design()
+    op = GridOperator(p.omega, p.dxes, p.epsilon, device=cuda)
+    E, info = op.solve(p.J, method=method, rtol=1e-8, criterion='true')
+    assert info.converged, info
+    A0 = O.e_full_csr(p.omega, p.dxes, p.epsilon)
+    b0 = -1j * p.omega * p.J
+    host = numpy.linalg.norm(A0 @ E.cpu().numpy() - b0) / numpy.linalg.norm(b0)
+    assert abs(host - info.residual) <= 1e-3 * host, (host, info.residual)
+    assert host <= 1e-8 and info.residual <= 1e-8
+
+
 def test_warm_start_and_history(cuda):
     from meanas_b200 import workloads
     from meanas_b200.operators import GridOperator

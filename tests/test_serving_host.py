@@ -14,7 +14,7 @@ from meanas_b200 import serving
 class FakeSlot:
     created = []
 
-    def __init__(self, shape, req, device, precision, xchunk):
+    def __init__(self, shape, req, device, precision, xchunk, autotune=True):
         self.shape = shape
         self.bytes = serving.slot_bytes(shape, precision)
         self.closed = False
@@ -38,6 +38,7 @@ def _server(budget, max_active, run_time=0.02):
     srv.rtol = 1e-8
     srv.maxiter = None
     srv.xchunk = None
+    srv.autotune = False
     srv._method = 'mixed'
     srv._cv = threading.Condition()
     srv._waiting = serving.collections.deque()
