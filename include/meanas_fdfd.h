@@ -295,8 +295,9 @@ int fdfd_fdtd_update_e(const fdfd_fdtd_desc* desc, void* E, const void* H, void*
  * (an exhausted or frozen allocator, or a host program that owns every device buffer
  * and can pass only inputs and outputs).  No counterpart in the reference.
  * The reduction scratch is a fixed 1 MiB array inside the library, held by every
- * device that loads it until exit; grids needing more than 32752 CTAs are rejected
- * with FDFD_ERR_ARG.  The first call on a device looks up that array's device
+ * device that loads it until exit; grids needing more than 32752 partial sums (one per
+ * 8-plane block of a 32 x 8 y/z tile, about 2048 cells each) are rejected with
+ * FDFD_ERR_ARG.  The first call on a device looks up that array's device
  * address; make it before any stream capture.  All calls share the array: calls
  * whose work overlaps on the GPU (other streams, other threads) race on it.
  * Like fdfd_residual, the four results pass through the plan's pinned host state:

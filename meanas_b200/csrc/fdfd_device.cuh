@@ -177,22 +177,43 @@ __device__ __forceinline__ double block_sum_n(double (&v)[NRED], double* sh) {
   return s;
 }
 
-// Reduce NRED per-thread accumulators across the grid; returns true in the one
-// thread (thread 0 of the last CTA) that holds the final sums in `out`.  Partials are
-// [CTA][NRED]; the last CTA reads them with independent loads (no per-value passes), so
-// the serial tail after the last CTA's own work is about two L2 round trips.
+// Warp 0 turns the per-thread sums of a plane block (sh[r * NT + t]) into partial number
+// `part`: lane l adds threads l, l + 32, ... in order, then a fixed shuffle tree.
 template <int NT, int NRED, typename A>
-__device__ bool grid_reduce(const A (&acc)[NRED], RedBuf rb, double* sh, double* out) {
+__device__ __forceinline__ void sum_block_partials(const A* sh, RedBuf rb, size_t part) {
+  const int lane = threadIdx.x + threadIdx.y * blockDim.x;  // called by threads 0..31
+#pragma unroll
+  for (int r = 0; r < NRED; ++r) {
+    double v = 0.0;
+#pragma unroll
+    for (int t = lane; t < NT; t += 32) v += (double)sh[r * NT + t];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) rb.partials[part * NRED + r] = v;
+  }
+}
+
+// Write the CTA's sum of NRED per-thread accumulators as partial number `part`
+// (threads r < NRED store value r).  Every thread of the CTA must call it.
+template <int NT, int NRED, typename A>
+__device__ __forceinline__ void write_partial(const A (&acc)[NRED], RedBuf rb, size_t part, double* sh) {
   const int tid = threadIdx.x + threadIdx.y * blockDim.x;
-  __shared__ bool s_last;
   double v[NRED];
 #pragma unroll
   for (int r = 0; r < NRED; ++r) v[r] = (double)acc[r];
-  const double part = block_sum_n<NT, NRED>(v, sh);
-  if (tid < NRED) {
-    rb.partials[(size_t)blockIdx.x * NRED + tid] = part;
-    __threadfence();
-  }
+  const double s = block_sum_n<NT, NRED>(v, sh);
+  if (tid < NRED) rb.partials[part * NRED + tid] = s;
+}
+
+// After every CTA has written its partials: the last CTA to arrive (atomic ticket) sums
+// all `nparts` partials in a fixed order and returns true in its thread 0, which holds
+// the totals in `out`.  The last CTA reads them with independent loads (no per-value
+// passes), so the serial tail after the last CTA's own work is about two L2 round trips.
+template <int NT, int NRED>
+__device__ bool grid_finish(RedBuf rb, unsigned int nparts, double* sh, double* out) {
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  __shared__ bool s_last;
+  __threadfence();
   __syncthreads();
   if (tid == 0) {
     __threadfence();  // cumulative: the partials written before the barrier are visible first
@@ -202,12 +223,11 @@ __device__ bool grid_reduce(const A (&acc)[NRED], RedBuf rb, double* sh, double*
   __syncthreads();
   if (!s_last) return false;
   __threadfence();
-  const unsigned int nb = gridDim.x;
   double s[NRED];
 #pragma unroll
   for (int r = 0; r < NRED; ++r) s[r] = 0.0;
 #pragma unroll 4
-  for (unsigned int b = tid; b < nb; b += NT) {
+  for (unsigned int b = tid; b < nparts; b += NT) {
 #pragma unroll
     for (int r = 0; r < NRED; ++r) s[r] += __ldcg(&rb.partials[(size_t)b * NRED + r]);
   }
@@ -221,6 +241,14 @@ __device__ bool grid_reduce(const A (&acc)[NRED], RedBuf rb, double* sh, double*
     *rb.ticket = 0u;
   }
   return tid == 0;
+}
+
+// Reduce NRED per-thread accumulators across the grid with one partial per CTA; returns
+// true in the one thread (thread 0 of the last CTA) that holds the final sums in `out`.
+template <int NT, int NRED, typename A>
+__device__ bool grid_reduce(const A (&acc)[NRED], RedBuf rb, double* sh, double* out) {
+  write_partial<NT, NRED>(acc, rb, blockIdx.x, sh);
+  return grid_finish<NT, NRED>(rb, gridDim.x, sh, out);
 }
 
 // Ops that carry solver state (a member `st` pointing to it) run finish() on a copy:
@@ -297,6 +325,11 @@ __device__ __forceinline__ void cp_async_cx(cx<R>* s, const cx<R>* g) {
 
 // Upper bound on x planes per CTA (per-CTA plane tables live in shared memory).
 constexpr int XC_MAX = 64;
+// Stencil reductions are summed over a fixed partition of the grid: one partial per
+// (block of RED_PLANES x planes, y/z tile), whatever the x chunk of the CTAs (chunks are
+// whole blocks), so the sums, and the Krylov iterates built on them, do not depend on
+// the tiling.
+constexpr int RED_PLANES = 8;
 
 template <typename R, int TZ, int TY, bool FLAT, int NB, int NO>
 struct StencilShape {
@@ -315,7 +348,9 @@ struct StencilShape {
   static constexpr size_t off_xt = off_h + sizeof(cx<R>) * (size_t)3 * HH * HW;
   static constexpr int XT_STRIDE = 6;  // per plane: idxe, idxh, dxe, dxh, (|dxe|, |dxh|)
   static constexpr size_t off_red = off_xt + sizeof(cx<R>) * (size_t)XT_STRIDE * (XC_MAX + 1);
-  static constexpr size_t smem_bytes() { return off_red + 64 * sizeof(double); }
+  // per-thread sums of a finished plane block ([NRED][NT], in the accumulator type)
+  static constexpr size_t off_blk = off_red + 64 * sizeof(double);
+  static constexpr size_t smem_bytes(int nred) { return off_blk + (size_t)nred * NT * sizeof(R); }
   static_assert(NHALO <= NT, "halo larger than the CTA");
 };
 
@@ -331,6 +366,8 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
   cx<R>* Hs = reinterpret_cast<cx<R>*>(smem_raw + S::off_h);        // [3][HH*HW]
   cx<R>* Xt = reinterpret_cast<cx<R>*>(smem_raw + S::off_xt);       // [XC+1][6]
   double* shred = reinterpret_cast<double*>(smem_raw + S::off_red);
+  using A = typename AccT<R>::type;
+  A* shblk = reinterpret_cast<A*>(smem_raw + S::off_blk);         // [NRED][NT]
 
   if (op.skip()) return;
   Op o = op;
@@ -404,10 +441,18 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
   WeightYZ<R> wyz;
   if (Op::NEEDS_W) wyz.init(g, jc, kc);
 
-  using A = typename AccT<R>::type;
-  A acc[Op::NRED > 0 ? Op::NRED : 1];
+  constexpr int NR = Op::NRED > 0 ? Op::NRED : 1;
+  // acc: the current plane block; accn: convert_own terms of plane i+1, converted one step
+  // ahead (folded into acc at the end of step i, or carried into the next block)
+  A acc[NR], accn[NR];
 #pragma unroll
-  for (int r = 0; r < (Op::NRED > 0 ? Op::NRED : 1); ++r) acc[r] = A(0);
+  for (int r = 0; r < NR; ++r) acc[r] = accn[r] = A(0);
+  // Partial of plane block `blk` (a block's warp sums wait in shred for the next barrier).
+  // The tile number is recomputed from blockIdx where it is needed: no registers held.
+  auto part_of = [&](int blk) -> size_t {
+    const int bt = (int)(blockIdx.x % (unsigned)(g.ntz * g.nty));
+    return (size_t)blk * (size_t)(g.ntz * g.nty) + (size_t)bt;
+  };
 
   // issue the asynchronous copies of plane iw's box inputs into Sbox
   auto issue = [&](int iw) {
@@ -441,7 +486,7 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
   };
   // convert the landed raw inputs of plane iw into U[buf]; own cells of the CTA's own
   // planes (own_plane) also run the op's convert_own
-  auto convert = [&](int buf, int iw, bool own_plane) {
+  auto convert = [&](int buf, int iw, bool own_plane, A* acc_to) {
     const int base = (int)iw * YZ;
 #pragma unroll
     for (int sl = 0; sl < 2; ++sl) {
@@ -462,7 +507,7 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
           cx<R> ov[NO > 0 ? NO : 1];
 #pragma unroll
           for (int oi = 0; oi < NO; ++oi) ov[oi] = Sown[(oi * 3 + c) * NT + tid];
-          o.convert_own(v, ov, idx, c, u, acc);
+          o.convert_own(v, ov, idx, c, u, acc_to);
         }
       }
     }
@@ -513,10 +558,10 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
   // (own slots only until the barrier: the barrier publishes Xt, U[0] and U[1])
   issue(ip);
   cp_async_wait_all();
-  convert(0, ip, false);
+  convert(0, ip, false, acc);
   issue(x0);
   cp_async_wait_all();
-  convert(1, x0, true);
+  convert(1, x0, true, acc);
   __syncthreads();
   // plane x0+1 starts landing while the prologue H is computed
   issue(x0 + 1 == g.X ? 0 : x0 + 1);
@@ -550,8 +595,14 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
     // converts only its own Sbox/Sown slots, U[nxt] (plane i-1) was last read before the
     // previous step's Hs barrier, and Hs is rewritten only after the barrier below.
     cp_async_wait_all();
-    convert(nxt, in1, i + 1 < x1);
+    const bool block_end = ((i + 1) % RED_PLANES == 0) || (i + 1 == x1);
+    convert(nxt, in1, i + 1 < x1, accn);
     __syncthreads();       // U[nxt] = u(i+1) ready for the neighbours' differences
+    if constexpr (Op::NRED > 0) {
+      // plane i-1 ended a block (chunks start on block boundaries): its per-thread sums
+      // are visible now; warp 0 adds them up in a fixed order
+      if (i > x0 && i % RED_PLANES == 0 && tid < 32) sum_block_partials<NT, Op::NRED>(shblk, rb, part_of(i / RED_PLANES - 1));
+    }
     if (i + 1 < x1) issue(in1 + 1 == g.X ? 0 : in1 + 1);
     const cx<R>* xe = Xt + (i - x0 + 1) * S::XT_STRIDE;
     const cx<R> idxe_i = xe[0], idxh_i = xe[1];
@@ -611,13 +662,30 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
       if (Op::NEEDS_W) wyz.at(xe[2], xe[3], xe[4].re, xe[4].im, W, aW);
       o.own(cell, i, j, k, u, y, W, aW, pr, acc);
     }
+    if constexpr (Op::NRED > 0) {
+      if (block_end) {  // uniform over the CTA
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+          shblk[r * NT + tid] = acc[r];
+          acc[r] = accn[r];
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) acc[r] += accn[r];
+      }
+#pragma unroll
+      for (int r = 0; r < NR; ++r) accn[r] = A(0);
+    }
     cur = nxt;
   }
   cp_async_wait_all();
 
   if constexpr (Op::NRED > 0) {
+    __syncthreads();  // the last block's per-thread sums (plane x1 - 1 always ends a block)
+    if (tid < 32) sum_block_partials<NT, Op::NRED>(shblk, rb, part_of((x1 - 1) / RED_PLANES));
     double sums[Op::NRED];
-    if (grid_reduce<NT, Op::NRED>(acc, rb, shred, sums)) run_finish(o, sums);
+    const unsigned int nparts = (unsigned int)((g.X + RED_PLANES - 1) / RED_PLANES) * (unsigned int)(g.ntz * g.nty);
+    if (grid_finish<NT, Op::NRED>(rb, nparts, shred, sums)) run_finish(o, sums);
   }
 }
 

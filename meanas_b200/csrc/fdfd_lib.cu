@@ -207,6 +207,8 @@ static Tiling make_tiling(const fdfd_plan* P, int precision) {
     long long need = (P->X * tiles + target - 1) / target;
     xc = (int)std::max(4LL, std::min(64LL, need));
   }
+  // whole blocks of the reductions' fixed plane partition per CTA (the last may be short)
+  xc = (xc + RED_PLANES - 1) / RED_PLANES * RED_PLANES;
   xc = std::min(std::min(xc, P->X), XC_MAX);
   t.XC = xc;
   t.nxc = (P->X + xc - 1) / xc;
@@ -222,6 +224,11 @@ static Geo<R> geo_with(const Geo<R>& g, const Tiling& t) {
   r.nty = t.nty;
   r.nxc = t.nxc;
   return r;
+}
+
+// Partial sums of one stencil reduction: one per (block of RED_PLANES x planes, tile).
+static long long stencil_parts(const fdfd_plan* P, const Tiling& t) {
+  return (long long)((P->X + RED_PLANES - 1) / RED_PLANES) * t.ntz * t.nty;
 }
 
 static long long max_blocks(const fdfd_plan* P) {
@@ -261,13 +268,13 @@ static int launch_stencil(fdfd_plan* P, const Geo<R>& g0, int precision, const O
   if (P->flat) {
     using Sh = StencilShape<R, 1, FLAT_TY, true, Op::NB, Op::NO>;
     auto kern = k_stencil<R, 1, FLAT_TY, true, MinBlocks<R>::value, Op>;
-    if (int rc = ensure_smem(kern, Sh::smem_bytes())) return rc;
-    kern<<<(unsigned)t.nblocks, dim3(1, FLAT_TY), Sh::smem_bytes(), s>>>(g, op, rb);
+    if (int rc = ensure_smem(kern, Sh::smem_bytes(Op::NRED))) return rc;
+    kern<<<(unsigned)t.nblocks, dim3(1, FLAT_TY), Sh::smem_bytes(Op::NRED), s>>>(g, op, rb);
   } else {
     using Sh = StencilShape<R, TZ3, TY3, false, Op::NB, Op::NO>;
     auto kern = k_stencil<R, TZ3, TY3, false, MinBlocks<R>::value, Op>;
-    if (int rc = ensure_smem(kern, Sh::smem_bytes())) return rc;
-    kern<<<(unsigned)t.nblocks, dim3(TZ3, TY3), Sh::smem_bytes(), s>>>(g, op, rb);
+    if (int rc = ensure_smem(kern, Sh::smem_bytes(Op::NRED))) return rc;
+    kern<<<(unsigned)t.nblocks, dim3(TZ3, TY3), Sh::smem_bytes(Op::NRED), s>>>(g, op, rb);
   }
   P->launches++;
   CKL();
@@ -1419,14 +1426,15 @@ static int static_scratch_address(void** out) {
 
 extern "C" int fdfd_residual_static(fdfd_plan* P, const void* E, const void* J, double out[4], void* stream) {
   if (!P || !E || !J || !out) return set_err(FDFD_ERR_ARG, "fdfd_residual_static: NULL argument");
-  // scratch layout: [0, 256) ticket, [256, 512) the four sums, [512, ...) per-CTA partials
+  // scratch layout: [0, 256) ticket, [256, 512) the four sums, [512, ...) partial sums
   const Tiling t = make_tiling(P, 0);
-  const size_t need = 512 + (size_t)t.nblocks * OpResidual<double>::NRED * sizeof(double);
+  const long long parts = stencil_parts(P, t);
+  const size_t need = 512 + (size_t)parts * OpResidual<double>::NRED * sizeof(double);
   if (need > STATIC_SCRATCH_BYTES)
     return set_err(FDFD_ERR_ARG,
-                   "fdfd_residual_static: the grid needs %lld CTAs (%zu scratch bytes); the fixed scratch holds "
-                   "%zu bytes (at most %zu CTAs) -- use fdfd_residual with a workspace",
-                   (long long)t.nblocks, need, STATIC_SCRATCH_BYTES,
+                   "fdfd_residual_static: the grid needs %lld partial sums (%zu scratch bytes); the fixed scratch "
+                   "holds %zu bytes (at most %zu partial sums) -- use fdfd_residual with a workspace",
+                   parts, need, STATIC_SCRATCH_BYTES,
                    (STATIC_SCRATCH_BYTES - 512) / (OpResidual<double>::NRED * sizeof(double)));
   void* base = nullptr;
   TRY(static_scratch_address(&base));
