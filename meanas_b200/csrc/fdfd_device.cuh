@@ -97,6 +97,7 @@ struct Geo {
   const R* muinv;        // 3N or null
   const uint8_t* mask;   // N or null
   const cx<R>* w2p;      // omega^2, in device memory (so captured graphs survive a new omega)
+  int rb_shift;          // reduction blocks of 2^rb_shift x planes (see stencil_unit)
 };
 
 __device__ __forceinline__ int wrapi(int v, int n) {
@@ -326,10 +327,10 @@ __device__ __forceinline__ void cp_async_cx(cx<R>* s, const cx<R>* g) {
 // Upper bound on x planes per CTA (per-CTA plane tables live in shared memory).
 constexpr int XC_MAX = 64;
 // Stencil reductions are summed over a fixed partition of the grid: one partial per
-// (block of RED_PLANES x planes, y/z tile), whatever the x chunk of the CTAs (chunks are
+// (block of 2^rb_shift x planes, y/z tile), whatever the x chunk of the CTAs (chunks are
 // whole blocks), so the sums, and the Krylov iterates built on them, do not depend on
-// the tiling.
-constexpr int RED_PLANES = 8;
+// the tiling.  The block size is a property of the grid (Geo::rb_shift): 8 planes, or 4
+// on small grids, where x chunks of 4 planes keep more SMs busy.
 
 template <typename R, int TZ, int TY, bool FLAT, int NB, int NO>
 struct StencilShape {
@@ -354,28 +355,27 @@ struct StencilShape {
   static_assert(NHALO <= NT, "halo larger than the CTA");
 };
 
-template <typename R, int TZ, int TY, bool FLAT, int MINB, class Op>
-__global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op, RedBuf rb) {
+// One work unit of a stencil pass: the x chunk `unit / (ntz * nty)` of the y/z tile
+// `unit % (ntz * nty)`.  Writes the unit's reduction partials (one per plane block); the
+// grid-wide sum and the op's finish() are the caller's.
+template <typename R, int TZ, int TY, bool FLAT, class Op>
+__device__ __forceinline__ void stencil_unit(const Geo<R>& g, const Op& o, RedBuf rb, int unit,
+                                             unsigned char* smem_raw) {
   using S = StencilShape<R, TZ, TY, FLAT, Op::NB, Op::NO>;
   constexpr int NT = S::NT, BW = S::BW, BOX = S::BOX, KZ = S::KZ, HW = S::HW, HH = S::HH;
   constexpr int NB = Op::NB, NO = Op::NO;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* Sbox = reinterpret_cast<cx<R>*>(smem_raw);                 // [NB][3][BOX]
   cx<R>* Sown = reinterpret_cast<cx<R>*>(smem_raw + S::off_own);    // [NO][3][NT]
   cx<R>* U = reinterpret_cast<cx<R>*>(smem_raw + S::off_u);         // [2][3][BOX]
   cx<R>* Hs = reinterpret_cast<cx<R>*>(smem_raw + S::off_h);        // [3][HH*HW]
   cx<R>* Xt = reinterpret_cast<cx<R>*>(smem_raw + S::off_xt);       // [XC+1][6]
-  double* shred = reinterpret_cast<double*>(smem_raw + S::off_red);
   using A = typename AccT<R>::type;
   A* shblk = reinterpret_cast<A*>(smem_raw + S::off_blk);         // [NRED][NT]
 
-  if (op.skip()) return;
-  Op o = op;
-  o.prepare();
   const cx<R> w2 = *g.w2p;
 
   const int tz = threadIdx.x, ty = threadIdx.y, tid = tz + ty * TZ;
-  int b = blockIdx.x;
+  int b = unit;
   const int tzb = b % g.ntz; b /= g.ntz;
   const int tyb = b % g.nty;
   const int xcb = b / g.nty;
@@ -450,7 +450,7 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
   // Partial of plane block `blk` (a block's warp sums wait in shred for the next barrier).
   // The tile number is recomputed from blockIdx where it is needed: no registers held.
   auto part_of = [&](int blk) -> size_t {
-    const int bt = (int)(blockIdx.x % (unsigned)(g.ntz * g.nty));
+    const int bt = unit % (g.ntz * g.nty);
     return (size_t)blk * (size_t)(g.ntz * g.nty) + (size_t)bt;
   };
 
@@ -595,13 +595,15 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
     // converts only its own Sbox/Sown slots, U[nxt] (plane i-1) was last read before the
     // previous step's Hs barrier, and Hs is rewritten only after the barrier below.
     cp_async_wait_all();
-    const bool block_end = ((i + 1) % RED_PLANES == 0) || (i + 1 == x1);
+    const int rbm = (1 << g.rb_shift) - 1;
+    const bool block_end = ((i + 1) & rbm) == 0 || (i + 1 == x1);
     convert(nxt, in1, i + 1 < x1, accn);
     __syncthreads();       // U[nxt] = u(i+1) ready for the neighbours' differences
     if constexpr (Op::NRED > 0) {
       // plane i-1 ended a block (chunks start on block boundaries): its per-thread sums
       // are visible now; warp 0 adds them up in a fixed order
-      if (i > x0 && i % RED_PLANES == 0 && tid < 32) sum_block_partials<NT, Op::NRED>(shblk, rb, part_of(i / RED_PLANES - 1));
+      if (i > x0 && (i & ((1 << g.rb_shift) - 1)) == 0 && tid < 32)
+        sum_block_partials<NT, Op::NRED>(shblk, rb, part_of((i >> g.rb_shift) - 1));
     }
     if (i + 1 < x1) issue(in1 + 1 == g.X ? 0 : in1 + 1);
     const cx<R>* xe = Xt + (i - x0 + 1) * S::XT_STRIDE;
@@ -682,10 +684,28 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
 
   if constexpr (Op::NRED > 0) {
     __syncthreads();  // the last block's per-thread sums (plane x1 - 1 always ends a block)
-    if (tid < 32) sum_block_partials<NT, Op::NRED>(shblk, rb, part_of((x1 - 1) / RED_PLANES));
+    if (tid < 32) sum_block_partials<NT, Op::NRED>(shblk, rb, part_of((x1 - 1) >> g.rb_shift));
+  }
+}
+
+// Partial sums of a stencil reduction: one per (plane block, tile).
+template <typename R>
+__device__ __forceinline__ unsigned int stencil_nparts(const Geo<R>& g) {
+  return (unsigned int)((g.X + (1 << g.rb_shift) - 1) >> g.rb_shift) * (unsigned int)(g.ntz * g.nty);
+}
+
+template <typename R, int TZ, int TY, bool FLAT, int MINB, class Op>
+__global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op, RedBuf rb) {
+  using S = StencilShape<R, TZ, TY, FLAT, Op::NB, Op::NO>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (op.skip()) return;
+  Op o = op;
+  o.prepare();
+  stencil_unit<R, TZ, TY, FLAT, Op>(g, o, rb, blockIdx.x, smem_raw);
+  if constexpr (Op::NRED > 0) {
     double sums[Op::NRED];
-    const unsigned int nparts = (unsigned int)((g.X + RED_PLANES - 1) / RED_PLANES) * (unsigned int)(g.ntz * g.nty);
-    if (grid_finish<NT, Op::NRED>(rb, nparts, shred, sums)) run_finish(o, sums);
+    double* shred = reinterpret_cast<double*>(smem_raw + S::off_red);
+    if (grid_finish<S::NT, Op::NRED>(rb, stencil_nparts(g), shred, sums)) run_finish(o, sums);
   }
 }
 
@@ -696,20 +716,11 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
 // SM streams to the end instead of idling through a partial last wave.
 //   void point(int cell, int i, int j, int k, const cx<R> W[3], const R aW[3], A* acc);
 template <typename R, int TZ, int TY, class Op>
-__global__ void __launch_bounds__(TZ * TY) k_point(const Geo<R> g, Op op, RedBuf rb) {
-  constexpr int NT = TZ * TY;
-  __shared__ double shred[64];
-  if (op.skip()) return;
-  Op o = op;
-  o.prepare();
+__device__ __forceinline__ void point_units(const Geo<R>& g, const Op& o, typename AccT<R>::type* acc) {
   const int tz = threadIdx.x, ty = threadIdx.y;
   const int ntiles = g.ntz * g.nty;
   const int units = ntiles * g.X;
   const int YZ = g.Y * g.Z;
-  using A = typename AccT<R>::type;
-  A acc[Op::NRED > 0 ? Op::NRED : 1];
-#pragma unroll
-  for (int r = 0; r < (Op::NRED > 0 ? Op::NRED : 1); ++r) acc[r] = A(0);
   for (int u = blockIdx.x; u < units; u += gridDim.x) {
     const int i = u / ntiles, t = u - i * ntiles;
     const int tyb = t / g.ntz, tzb = t - tyb * g.ntz;
@@ -725,6 +736,20 @@ __global__ void __launch_bounds__(TZ * TY) k_point(const Geo<R> g, Op op, RedBuf
       o.point(i * YZ + j * g.Z + k, i, j, k, W, aW, acc);
     }
   }
+}
+
+template <typename R, int TZ, int TY, class Op>
+__global__ void __launch_bounds__(TZ * TY) k_point(const Geo<R> g, Op op, RedBuf rb) {
+  constexpr int NT = TZ * TY;
+  __shared__ double shred[64];
+  if (op.skip()) return;
+  Op o = op;
+  o.prepare();
+  using A = typename AccT<R>::type;
+  A acc[Op::NRED > 0 ? Op::NRED : 1];
+#pragma unroll
+  for (int r = 0; r < (Op::NRED > 0 ? Op::NRED : 1); ++r) acc[r] = A(0);
+  point_units<R, TZ, TY, Op>(g, o, acc);
   if constexpr (Op::NRED > 0) {
     double sums[Op::NRED];
     // (finish runs on the global state here: a state copy would cost this kernel occupancy)

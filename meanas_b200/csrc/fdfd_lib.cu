@@ -124,6 +124,7 @@ struct fdfd_plan {
   bool flat;
   bool has32;
   int nsm;
+  int rb_shift;            // reductions over blocks of 2^rb_shift x planes (a grid property)
   int xc_override[2];
   Geo<double> g64;
   Geo<float> g32;
@@ -208,7 +209,8 @@ static Tiling make_tiling(const fdfd_plan* P, int precision) {
     xc = (int)std::max(4LL, std::min(64LL, need));
   }
   // whole blocks of the reductions' fixed plane partition per CTA (the last may be short)
-  xc = (xc + RED_PLANES - 1) / RED_PLANES * RED_PLANES;
+  const int rbp = 1 << P->rb_shift;
+  xc = (xc + rbp - 1) / rbp * rbp;
   xc = std::min(std::min(xc, P->X), XC_MAX);
   t.XC = xc;
   t.nxc = (P->X + xc - 1) / xc;
@@ -226,9 +228,10 @@ static Geo<R> geo_with(const Geo<R>& g, const Tiling& t) {
   return r;
 }
 
-// Partial sums of one stencil reduction: one per (block of RED_PLANES x planes, tile).
+// Partial sums of one stencil reduction: one per (block of 2^rb_shift x planes, tile).
 static long long stencil_parts(const fdfd_plan* P, const Tiling& t) {
-  return (long long)((P->X + RED_PLANES - 1) / RED_PLANES) * t.ntz * t.nty;
+  const int rbp = 1 << P->rb_shift;
+  return (long long)((P->X + rbp - 1) / rbp) * t.ntz * t.nty;
 }
 
 static long long max_blocks(const fdfd_plan* P) {
@@ -401,6 +404,7 @@ static void plan_fill(fdfd_plan* P, const fdfd_grid_desc* d, const PlanLayout& L
   }
   const int nb = (int)std::min<long long>((3 * N + 255) / 256, 148LL * 16);
   P->g64.eps = d->epsilon;
+  P->g64.rb_shift = P->g32.rb_shift = P->rb_shift;
   P->g64.muinv = nullptr;
   P->g32.muinv = nullptr;
   P->g32.eps = nullptr;
@@ -470,6 +474,8 @@ extern "C" int fdfd_plan_create(const fdfd_grid_desc* d, void* ws, size_t ws_byt
   P->flat = (P->Z == 1);
   P->has32 = (d->flags & FDFD_GRID_FP32) != 0;
   P->xc_override[0] = P->xc_override[1] = 0;
+  // reduction blocks of 8 x planes; 4 below 2M cells, where 4-plane chunks keep more SMs busy
+  P->rb_shift = P->N >= (1LL << 21) ? 3 : 2;
   int dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&P->nsm, cudaDevAttrMultiProcessorCount, dev);

@@ -192,8 +192,9 @@ class GridOperator:
         return self._plan
 
     def set_xchunk(self, precision: str, xchunk: int) -> None:
-        """Override the x planes per CTA (autotuning hook; rounded up to whole 8-plane
-        blocks of the reductions' fixed partition); 0 restores the default."""
+        """Override the x planes per CTA (autotuning hook; rounded up to whole blocks of the
+        reductions' fixed plane partition: 8 planes, 4 below 2M cells); 0 restores the
+        default."""
         _lib.check(self.lib.fdfd_plan_set_xchunk(self.plan, _PREC[precision], int(xchunk)))
 
     # ------------------------------------------------------------------ products
@@ -316,8 +317,10 @@ class GridOperator:
         size on the same device start from it.  Returns {precision: (xchunk, us/iteration, all)}."""
         X = self.shape[0]
         if candidates is None:
-            # whole blocks of the reductions' 8-plane partition (the library rounds up to them)
-            candidates = sorted({c for c in (8, 16, 24, 32, 40, 48, 56, 64) if c <= max(8, X)} | {min(X, 64)})
+            # whole blocks of the reductions' plane partition (8 planes, 4 below 2M cells;
+            # the library rounds up to them)
+            step = 8 if self.n_cells >= 1 << 21 else 4
+            candidates = sorted({c for c in range(step, 65, step) if c <= max(step, X)} | {min(X, 64)})
         g = torch.Generator(device=self.device).manual_seed(1)
         J = torch.zeros(self.n, dtype=torch.complex128, device=self.device)
         J[self.n // 2] = 1.0
