@@ -326,11 +326,15 @@ __device__ __forceinline__ void cp_async_cx(cx<R>* s, const cx<R>* g) {
 
 // Upper bound on x planes per CTA (per-CTA plane tables live in shared memory).
 constexpr int XC_MAX = 64;
-// Stencil reductions are summed over a fixed partition of the grid: one partial per
-// (block of 2^rb_shift x planes, y/z tile), whatever the x chunk of the CTAs (chunks are
-// whole blocks), so the sums, and the Krylov iterates built on them, do not depend on
-// the tiling.  The block size is a property of the grid (Geo::rb_shift): 8 planes, or 4
-// on small grids, where x chunks of 4 planes keep more SMs busy.
+// Complex128 stencil reductions are summed over a fixed partition of the grid: one
+// partial per (block of 2^rb_shift x planes, y/z tile), whatever the x chunk of the CTAs
+// (chunks are whole blocks), so the sums, and the COCG iterates built on them, do not
+// depend on the tiling.  The block size is a property of the grid (Geo::rb_shift): 8
+// planes, or 4 on small grids, where x chunks of 4 planes keep more SMs busy.  Complex64
+// passes keep one partial per CTA: their per-thread FP32 sums already depend on the
+// order of the cells, and the per-block partials cost their short passes about 10 %.
+template <typename R>
+struct PartitionedSums : std::is_same<R, double> {};
 
 template <typename R, int TZ, int TY, bool FLAT, int NB, int NO>
 struct StencilShape {
@@ -351,7 +355,10 @@ struct StencilShape {
   static constexpr size_t off_red = off_xt + sizeof(cx<R>) * (size_t)XT_STRIDE * (XC_MAX + 1);
   // per-thread sums of a finished plane block ([NRED][NT], in the accumulator type)
   static constexpr size_t off_blk = off_red + 64 * sizeof(double);
-  static constexpr size_t smem_bytes(int nred) { return off_blk + (size_t)nred * NT * sizeof(R); }
+  // complex128 passes only (see PartitionedSums); complex64 passes keep one partial per CTA
+  static constexpr size_t smem_bytes(int nred) {
+    return off_blk + (std::is_same<R, double>::value ? (size_t)nred * NT * sizeof(R) : (size_t)0);
+  }
   static_assert(NHALO <= NT, "halo larger than the CTA");
 };
 
@@ -595,11 +602,13 @@ __device__ __forceinline__ void stencil_unit(const Geo<R>& g, const Op& o, RedBu
     // converts only its own Sbox/Sown slots, U[nxt] (plane i-1) was last read before the
     // previous step's Hs barrier, and Hs is rewritten only after the barrier below.
     cp_async_wait_all();
+    constexpr bool PART = PartitionedSums<R>::value && Op::NRED > 0;
     const int rbm = (1 << g.rb_shift) - 1;
     const bool block_end = ((i + 1) & rbm) == 0 || (i + 1 == x1);
-    convert(nxt, in1, i + 1 < x1, accn);
+    if constexpr (PART) convert(nxt, in1, i + 1 < x1, accn);
+    else convert(nxt, in1, i + 1 < x1, acc);
     __syncthreads();       // U[nxt] = u(i+1) ready for the neighbours' differences
-    if constexpr (Op::NRED > 0) {
+    if constexpr (PART) {
       // plane i-1 ended a block (chunks start on block boundaries): its per-thread sums
       // are visible now; warp 0 adds them up in a fixed order
       if (i > x0 && (i & ((1 << g.rb_shift) - 1)) == 0 && tid < 32)
@@ -664,7 +673,7 @@ __device__ __forceinline__ void stencil_unit(const Geo<R>& g, const Op& o, RedBu
       if (Op::NEEDS_W) wyz.at(xe[2], xe[3], xe[4].re, xe[4].im, W, aW);
       o.own(cell, i, j, k, u, y, W, aW, pr, acc);
     }
-    if constexpr (Op::NRED > 0) {
+    if constexpr (PART) {
       if (block_end) {  // uniform over the CTA
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
@@ -683,8 +692,12 @@ __device__ __forceinline__ void stencil_unit(const Geo<R>& g, const Op& o, RedBu
   cp_async_wait_all();
 
   if constexpr (Op::NRED > 0) {
-    __syncthreads();  // the last block's per-thread sums (plane x1 - 1 always ends a block)
-    if (tid < 32) sum_block_partials<NT, Op::NRED>(shblk, rb, part_of((x1 - 1) >> g.rb_shift));
+    if constexpr (PartitionedSums<R>::value) {
+      __syncthreads();  // the last block's per-thread sums (plane x1 - 1 always ends a block)
+      if (tid < 32) sum_block_partials<NT, Op::NRED>(shblk, rb, part_of((x1 - 1) >> g.rb_shift));
+    } else {
+      write_partial<NT, Op::NRED>(acc, rb, (size_t)unit, reinterpret_cast<double*>(smem_raw + S::off_red));
+    }
   }
 }
 
@@ -705,7 +718,8 @@ __global__ void __launch_bounds__(TZ * TY, MINB) k_stencil(const Geo<R> g, Op op
   if constexpr (Op::NRED > 0) {
     double sums[Op::NRED];
     double* shred = reinterpret_cast<double*>(smem_raw + S::off_red);
-    if (grid_finish<S::NT, Op::NRED>(rb, stencil_nparts(g), shred, sums)) run_finish(o, sums);
+    const unsigned int nparts = PartitionedSums<R>::value ? stencil_nparts(g) : gridDim.x;
+    if (grid_finish<S::NT, Op::NRED>(rb, nparts, shred, sums)) run_finish(o, sums);
   }
 }
 

@@ -208,9 +208,12 @@ static Tiling make_tiling(const fdfd_plan* P, int precision) {
     long long need = (P->X * tiles + target - 1) / target;
     xc = (int)std::max(4LL, std::min(64LL, need));
   }
-  // whole blocks of the reductions' fixed plane partition per CTA (the last may be short)
-  const int rbp = 1 << P->rb_shift;
-  xc = (xc + rbp - 1) / rbp * rbp;
+  // complex128: whole blocks of the reductions' fixed plane partition per CTA (the last
+  // may be short)
+  if (precision == 0) {
+    const int rbp = 1 << P->rb_shift;
+    xc = (xc + rbp - 1) / rbp * rbp;
+  }
   xc = std::min(std::min(xc, P->X), XC_MAX);
   t.XC = xc;
   t.nxc = (P->X + xc - 1) / xc;
@@ -684,7 +687,10 @@ static int drive(fdfd_plan* P, KState* d_st, int chunk, int maxiter, cudaStream_
   return 0;
 }
 
-// Capture `enqueue` (one batch) as a CUDA graph on the private stream, cached by key.
+// Capture `enqueue` (one batch) as a CUDA graph on the private stream, cached by key
+// (at most kMaxGraphs executables per plan).
+static constexpr size_t kMaxGraphs = 24;
+
 template <class Enq>
 static int graph_batch(fdfd_plan* P, int kind, const void* ka, const void* kb, int chunk, cudaStream_t s,
                        Enq enqueue) {
@@ -706,6 +712,13 @@ static int graph_batch(fdfd_plan* P, int kind, const void* ka, const void* kb, i
   e = cudaGraphInstantiate(&ex, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return set_err(FDFD_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+  // bounded cache: a long-lived plan that solves into fresh output buffers would otherwise
+  // keep one executable per buffer address; the oldest entry goes first (its launches
+  // were enqueued on `s` earlier, and a graph may be destroyed while it runs)
+  if (P->graphs.size() >= kMaxGraphs) {
+    cudaGraphExecDestroy(P->graphs.front().exec);
+    P->graphs.erase(P->graphs.begin());
+  }
   P->graphs.push_back({kind, ka, kb, chunk, ex});
   CK(cudaGraphLaunch(ex, s));
   return 0;

@@ -192,9 +192,9 @@ class GridOperator:
         return self._plan
 
     def set_xchunk(self, precision: str, xchunk: int) -> None:
-        """Override the x planes per CTA (autotuning hook; rounded up to whole blocks of the
-        reductions' fixed plane partition: 8 planes, 4 below 2M cells); 0 restores the
-        default."""
+        """Override the x planes per CTA (autotuning hook; for complex128 rounded up to
+        whole blocks of the reductions' fixed plane partition: 8 planes, 4 below 2M cells);
+        0 restores the default."""
         _lib.check(self.lib.fdfd_plan_set_xchunk(self.plan, _PREC[precision], int(xchunk)))
 
     # ------------------------------------------------------------------ products
@@ -316,11 +316,16 @@ class GridOperator:
         such runs.  The choice is kept for the process: later operators of the same grid
         size on the same device start from it.  Returns {precision: (xchunk, us/iteration, all)}."""
         X = self.shape[0]
+        cands = {}
         if candidates is None:
-            # whole blocks of the reductions' plane partition (8 planes, 4 below 2M cells;
-            # the library rounds up to them)
+            # complex128: whole blocks of the reductions' plane partition (8 planes, 4 below
+            # 2M cells; the library rounds up to them); complex64: any chunk
             step = 8 if self.n_cells >= 1 << 21 else 4
-            candidates = sorted({c for c in range(step, 65, step) if c <= max(step, X)} | {min(X, 64)})
+            cands['c128'] = sorted({c for c in range(step, 65, step) if c <= max(step, X)} | {min(X, 64)})
+            cands['c64'] = sorted({c for c in (4, 5, 6, 8, 10, 11, 12, 14, 16, 20, 24, 28, 32, 40, 48, 64)
+                                   if c <= max(4, X)} | {min(X, 64)})
+        else:
+            cands['c128'] = cands['c64'] = list(candidates)
         g = torch.Generator(device=self.device).manual_seed(1)
         J = torch.zeros(self.n, dtype=torch.complex128, device=self.device)
         J[self.n // 2] = 1.0
@@ -332,7 +337,7 @@ class GridOperator:
                 continue
             kinds = (2, 3) if method == 'mixed' else (0, 1)
             timing = {}
-            for xc in candidates:
+            for xc in cands[prec]:
                 self.set_xchunk(prec, xc)
                 # one batch of exactly `iters` iterations, so few no-op launches follow the cap
                 kw = dict(method=method, rtol=1e-30, maxiter=iters, criterion='true', profile=True,

@@ -145,3 +145,19 @@ def test_sizes_mismatch_raise(cuda):
         generic(p.omega, p.dxes, p.J[:-3], p.epsilon, device=cuda)
     with pytest.raises(NotImplementedError):
         generic(p.omega, p.dxes, p.J, p.epsilon, matrix_solver=lambda A, b: b, device=cuda)
+
+
+def test_progress_logged_every_100_iterations_like_the_reference(cuda, caplog):
+    """meanas/fdfd/solvers.py:43-48 logs ||A x - b|| / ||b|| every 100 iterations at INFO on
+    the 'meanas.fdfd.solvers' logger; the drop-in logs the same lines after its solve."""
+    import logging
+    from meanas_b200 import generic, workloads
+    p = workloads.dipole_core(24, pml=6)
+    with caplog.at_level(logging.INFO, logger='meanas.fdfd.solvers'):
+        E, info = generic(p.omega, p.dxes, p.J, p.epsilon, matrix_solver_opts=dict(rtol=1e-8),
+                          return_info=True, device=cuda)
+    lines = [r.getMessage() for r in caplog.records if r.name == 'meanas.fdfd.solvers']
+    assert info.converged and info.iterations >= 200
+    assert len(lines) == info.iterations // 100
+    assert lines[0].startswith('Solver residual at iteration 100 : ')
+    assert float(lines[0].split(':')[-1]) == pytest.approx(info.history[100], rel=1e-12)
