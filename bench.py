@@ -511,11 +511,15 @@ def kernel_mode(args) -> None:
     else:
         p = workloads.BY_NAME[args.workload]()
     dev = torch.device('cuda', 0)
-    op = GridOperator(p.omega, p.dxes, p.epsilon, p.mu, p.pec, p.pmc, device=dev, fp32=True)
+    blocks = set(args.kernel_blocks.split(','))
     extra_c128 = (24 if p.mu is not None else 0) + (1 if p.pec is not None or p.pmc is not None else 0)
     extra_c64 = (12 if p.mu is not None else 0) + (1 if p.pec is not None or p.pmc is not None else 0)
-    J = torch.as_tensor(p.J, device=dev)
-    for method in ('cocg', 'mixed'):
+    x = torch.randn(p.n_unknowns, dtype=torch.complex128, device=dev)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if blocks & {'solvers', 'apply', 'fields'}:
+        op = GridOperator(p.omega, p.dxes, p.epsilon, p.mu, p.pec, p.pmc, device=dev, fp32=True)
+        J = torch.as_tensor(p.J, device=dev)
+    for method in (('cocg', 'mixed') if 'solvers' in blocks else ()):
         _, info = op.solve(J, method=method, rtol=1e-30, maxiter=args.kernel_iters, criterion='true',
                            profile=True, max_outer=1)
         for k in range(4):
@@ -525,8 +529,7 @@ def kernel_mode(args) -> None:
                 gbs = (KERNEL_BYTES_PER_CELL[k] + extra) * p.n_cells / (ms / 1e3) / 1e9
                 print(f'{method:6s} {KERNEL_NAMES[k]:20s} {info.kernel_count[k]:5d} launches  '
                       f'{ms * 1e3:8.1f} us  {gbs:7.1f} GB/s algorithmic')
-    x = torch.randn(p.n_unknowns, dtype=torch.complex128, device=dev)
-    for prec, xx in (('c128', x), ('c64', x.to(torch.complex64))):
+    for prec, xx in ((('c128', x), ('c64', x.to(torch.complex64))) if 'apply' in blocks else ()):
         for _ in range(3):
             op.apply(xx, precision=prec)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -542,43 +545,44 @@ def kernel_mode(args) -> None:
               f'{per_cell * p.n_cells / (ms / 1e3) / 1e9:7.1f} GB/s algorithmic')
     # E -> (H, E x conj(H)) in one pass: read E, write H and S (3 x 48 B per cell; mu and the
     # mask byte when present)
-    for _ in range(3):
-        op.poynting(x)
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record()
-    for _ in range(10):
-        op.poynting(x)
-    b.record()
-    torch.cuda.synchronize()
-    ms = a.elapsed_time(b) / 10
-    per_cell = 3 * 48 + (24 if p.mu is not None else 0) + (1 if p.pmc is not None else 0)
-    print(f'fields e2h+poynting c128         10 launches  {ms * 1e3:8.1f} us  '
-          f'{per_cell * p.n_cells / (ms / 1e3) / 1e9:7.1f} GB/s algorithmic')
+    if 'fields' in blocks:
+        for _ in range(3):
+            op.poynting(x)
+        a.record()
+        for _ in range(10):
+            op.poynting(x)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / 10
+        per_cell = 3 * 48 + (24 if p.mu is not None else 0) + (1 if p.pmc is not None else 0)
+        print(f'fields e2h+poynting c128         10 launches  {ms * 1e3:8.1f} us  '
+              f'{per_cell * p.n_cells / (ms / 1e3) / 1e9:7.1f} GB/s algorithmic')
     # CSR product of the matrix_solver hook on a matrix shaped like the assembled operator:
     # 3N rows, 13 nonzeros per row at the curl-curl stencil's column offsets (synthetic
     # values); bytes = values + column indices + row pointers + x once + y
-    # FDTD: one H + one E half step of the plain Yee updates on float32 fields (E step: read
-    # H, E, epsilon (float64), write E = 60 B/cell; H step: read E, H, write H = 36 B/cell)
-    from meanas_b200 import fdtd
-    rdx = [[numpy.abs(d).astype(float) for d in g] for g in p.dxes]
-    eh2h, eh2e = fdtd.maxwell_h(0.3, rdx, device=dev), fdtd.maxwell_e(0.3, rdx, device=dev)
-    ef = torch.randn((3, *p.shape), dtype=torch.float32, device=dev)
-    hf = torch.randn_like(ef)
-    epsf = torch.as_tensor(p.epsilon, device=dev)
-    for _ in range(3):
-        eh2h(ef, hf)
-        eh2e(ef, hf, epsf)
-    a.record()
-    for _ in range(10):
-        eh2h(ef, hf)
-        eh2e(ef, hf, epsf)
-    b.record()
-    torch.cuda.synchronize()
-    ms = a.elapsed_time(b) / 10
-    print(f'fdtd   H+E step f32                10 steps     {ms * 1e3:8.1f} us  '
-          f'{96 * p.n_cells / (ms / 1e3) / 1e9:7.1f} GB/s algorithmic')
-    del ef, hf
-    if p.n_unknowns > 12_000_000:
+    if 'fdtd' in blocks:
+        # FDTD: one H + one E half step of the plain Yee updates on float32 fields (E step: read
+        # H, E, epsilon (float64), write E = 60 B/cell; H step: read E, H, write H = 36 B/cell)
+        from meanas_b200 import fdtd
+        rdx = [[numpy.abs(d).astype(float) for d in g] for g in p.dxes]
+        eh2h, eh2e = fdtd.maxwell_h(0.3, rdx, device=dev), fdtd.maxwell_e(0.3, rdx, device=dev)
+        ef = torch.randn((3, *p.shape), dtype=torch.float32, device=dev)
+        hf = torch.randn_like(ef)
+        epsf = torch.as_tensor(p.epsilon, device=dev)
+        for _ in range(3):
+            eh2h(ef, hf)
+            eh2e(ef, hf, epsf)
+        a.record()
+        for _ in range(10):
+            eh2h(ef, hf)
+            eh2e(ef, hf, epsf)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / 10
+        print(f'fdtd   H+E step f32                10 steps     {ms * 1e3:8.1f} us  '
+              f'{96 * p.n_cells / (ms / 1e3) / 1e9:7.1f} GB/s algorithmic')
+        del ef, hf
+    if 'csr' not in blocks or p.n_unknowns > 12_000_000:
         return
     from scipy import sparse
     from meanas_b200.csr import CsrMatrix
@@ -765,6 +769,8 @@ def main():
     ap.add_argument('--kernel-iters', type=int, default=0,
                     help='profiling mode: run this many iterations of each solver (no convergence, no JSON)')
     ap.add_argument('--shape', type=int, nargs=3, default=None, help='profiling mode grid shape')
+    ap.add_argument('--kernel-blocks', default='solvers,apply,fields,fdtd,csr',
+                    help='profiling mode: which kernel groups to run (comma list)')
     ap.add_argument('--timed-profile', choices=['on', 'off'], default='off',
                     help='per-launch CUDA events inside the timed solves (off: graph launches, kernel '
                          'durations from one profiled solve after them)')
