@@ -518,6 +518,8 @@ def kernel_mode(args) -> None:
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if blocks & {'solvers', 'apply', 'fields'}:
         op = GridOperator(p.omega, p.dxes, p.epsilon, p.mu, p.pec, p.pmc, device=dev, fp32=True)
+        if args.xchunk:
+            op.set_xchunk('c128', args.xchunk)
         J = torch.as_tensor(p.J, device=dev)
     for method in (('cocg', 'mixed') if 'solvers' in blocks else ()):
         _, info = op.solve(J, method=method, rtol=1e-30, maxiter=args.kernel_iters, criterion='true',
@@ -769,6 +771,8 @@ def main():
     ap.add_argument('--kernel-iters', type=int, default=0,
                     help='profiling mode: run this many iterations of each solver (no convergence, no JSON)')
     ap.add_argument('--shape', type=int, nargs=3, default=None, help='profiling mode grid shape')
+    ap.add_argument('--xchunk', type=int, default=0,
+                    help='profiling mode: x planes per CTA of the complex128 passes (0: default tiling)')
     ap.add_argument('--kernel-blocks', default='solvers,apply,fields,fdtd,csr',
                     help='profiling mode: which kernel groups to run (comma list)')
     ap.add_argument('--timed-profile', choices=['on', 'off'], default='off',
