@@ -617,8 +617,8 @@ def gradient_check(args) -> dict:
     torch.autograd (one forward + one adjoint GPU solve), checked two ways:
 
     * against the reference's own adjoint gradient (tests/golden/grad96.npz: the reference
-      generic() forward solve and generic(adjoint=True) solve, scipy QMR to rtol 1e-10,
-      formed over the whole 40x40x8 design region);
+      generic() forward solve and generic(adjoint=True) solve with scipy QMR, formed over the
+      whole 40x40x8 design region);
     * against central finite differences of GPU FP64 solves (rtol `grad_rtol`) on `fd_cells`
       random design cells, Richardson-extrapolated from steps h and h/2
       ((4 D(h/2) - D(h)) / 3, truncation O(h^4)) so that a step large enough to keep the
@@ -663,7 +663,7 @@ def gradient_check(args) -> dict:
                                                                  numpy.abs(cell_gr)[sig])),
                 'significant_cells': int(sig.sum()), 'cells': int(sig.size),
                 'reference_loss': float(z['loss']), 'loss_rel_err': abs(L.item() - float(z['loss'])) / float(z['loss']),
-                'reference': 'reference generic() + generic(adjoint=True), scipy QMR rtol 1e-10 '
+                'reference': f'reference generic() + generic(adjoint=True), scipy QMR rtol {float(z["rtol"]):g} '
                              f'(iterations {z["qmr_iterations"].tolist()}, residuals {float(z["residual"]):.1e} / '
                              f'{float(z["residual_adjoint"]):.1e})'}
         else:

@@ -39,10 +39,12 @@ the only place that reads it.  Outputs:
                     own solves: ``generic()`` for E, ``generic(adjoint=True)`` with
                     ``-i omega J_adj = 2 E`` on the monitor plane, ``dL/deps =
                     Re(omega^2 conj(E_adj) E)`` over the 40x40x8 design region (not part of
-                    the default set: two QMR solves of 1.77M unknowns take a while).
+                    the default set: two QMR solves of 1.77M unknowns take hours; the QMR
+                    tolerance comes from GRAD96_RTOL, default 1e-10, and is stored).
 """
 from __future__ import annotations
 
+import os
 import sys
 import time
 from pathlib import Path
@@ -546,15 +548,21 @@ def gen_grad96() -> None:
     p = workloads.adjoint_design()
     its = []
 
+    t_start = time.perf_counter()
+
     def qmr_counting(A, b, **kw):
         it = [0]
 
         def cb(_):
             it[0] += 1
+            if it[0] % 1000 == 0:
+                print(f'grad96: solve {len(its) + 1}, QMR iteration {it[0]}, '
+                      f'{time.perf_counter() - t_start:.0f} s', flush=True)
         x = scipy.sparse.linalg.qmr(A, b, callback=cb, **kw)[0]
         its.append(it[0])
         return x
-    opts = dict(rtol=1e-10, atol=0)
+    # GRAD96_RTOL: the QMR tolerance of both solves (default 1e-10)
+    opts = dict(rtol=float(os.environ.get('GRAD96_RTOL', '1e-10')), atol=0)
     t0 = time.perf_counter()
     E = solvers.generic(p.omega, p.dxes, p.J, p.epsilon, matrix_solver=qmr_counting,
                         matrix_solver_opts=opts)
@@ -571,7 +579,7 @@ def gen_grad96() -> None:
     res = numpy.linalg.norm(A0 @ E - b0) / numpy.linalg.norm(b0)
     ba = -1j * p.omega * J_adj
     res_adj = numpy.linalg.norm(A0.conj().T @ E_adj - ba) / numpy.linalg.norm(ba)
-    numpy.savez_compressed(OUT / 'grad96.npz', grad_design=grad[(slice(None), *dsl)],
+    numpy.savez_compressed(OUT / os.environ.get('GRAD96_FILE', 'grad96.npz'), grad_design=grad[(slice(None), *dsl)],
                            eps_design=p.epsilon.reshape(3, *p.shape)[(slice(None), *dsl)],
                            loss=float(numpy.sum(numpy.abs(E[mon]) ** 2)), qmr_iterations=numpy.array(its),
                            seconds=t1 - t0, residual=res, residual_adjoint=res_adj, rtol=opts['rtol'])

@@ -62,7 +62,8 @@ GRAD96 = __import__('conftest').GOLDEN / 'grad96.npz'
 def test_autograd_gradient_matches_reference_adjoint_at_96(cuda):
     """The 96x96x64 design problem: dL/deps from torch.autograd (GPU forward + adjoint
     solves) against the reference's own gradient (its generic() and generic(adjoint=True)
-    solves, scipy QMR to rtol 1e-10) over the whole 40x40x8 design region."""
+    solves with scipy QMR, the tolerance stored in the file) over the whole 40x40x8 design
+    region."""
     import torch
     from meanas_b200 import workloads
     from meanas_b200.autograd import fdfd_solve
