@@ -41,6 +41,8 @@ the only place that reads it.  Outputs:
                     Re(omega^2 conj(E_adj) E)`` over the 40x40x8 design region (not part of
                     the default set: two QMR solves of 1.77M unknowns take hours; the QMR
                     tolerance comes from GRAD96_RTOL, default 1e-10, and is stored).
+* ``grad48.npz``    the same on the design problem scaled to 48x48x40 (``GRAD48``), whose two
+                    QMR solves take minutes.
 """
 from __future__ import annotations
 
@@ -545,7 +547,19 @@ def gen_modesrc() -> None:
 
 def gen_grad96() -> None:
     from meanas_b200 import workloads
-    p = workloads.adjoint_design()
+    _grad_fixture(workloads.adjoint_design(), os.environ.get('GRAD96_FILE', 'grad96.npz'))
+
+
+def gen_grad48() -> None:
+    from meanas_b200 import workloads
+    _grad_fixture(workloads.adjoint_design(**GRAD48), 'grad48.npz')
+
+
+# the 96x96x64 design problem scaled down (the reference's QMR solves take minutes)
+GRAD48 = dict(shape=(48, 48, 40), pml=8, wavelength=26.0, design=(16, 16, 6), source_x=12, monitor_x=36)
+
+
+def _grad_fixture(p, name: str) -> None:
     its = []
 
     t_start = time.perf_counter()
@@ -556,7 +570,7 @@ def gen_grad96() -> None:
         def cb(_):
             it[0] += 1
             if it[0] % 1000 == 0:
-                print(f'grad96: solve {len(its) + 1}, QMR iteration {it[0]}, '
+                print(f'{name}: solve {len(its) + 1}, QMR iteration {it[0]}, '
                       f'{time.perf_counter() - t_start:.0f} s', flush=True)
         x = scipy.sparse.linalg.qmr(A, b, callback=cb, **kw)[0]
         its.append(it[0])
@@ -579,11 +593,11 @@ def gen_grad96() -> None:
     res = numpy.linalg.norm(A0 @ E - b0) / numpy.linalg.norm(b0)
     ba = -1j * p.omega * J_adj
     res_adj = numpy.linalg.norm(A0.conj().T @ E_adj - ba) / numpy.linalg.norm(ba)
-    numpy.savez_compressed(OUT / os.environ.get('GRAD96_FILE', 'grad96.npz'), grad_design=grad[(slice(None), *dsl)],
+    numpy.savez_compressed(OUT / name, grad_design=grad[(slice(None), *dsl)],
                            eps_design=p.epsilon.reshape(3, *p.shape)[(slice(None), *dsl)],
                            loss=float(numpy.sum(numpy.abs(E[mon]) ** 2)), qmr_iterations=numpy.array(its),
                            seconds=t1 - t0, residual=res, residual_adjoint=res_adj, rtol=opts['rtol'])
-    print('grad96', its, t1 - t0, res, res_adj)
+    print(name, its, t1 - t0, res, res_adj)
 
 
 if __name__ == '__main__':

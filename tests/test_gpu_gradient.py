@@ -84,3 +84,32 @@ def test_autograd_gradient_matches_reference_adjoint_at_96(cuda):
     cg, cr = g.sum(axis=0), ref.sum(axis=0)
     sig = numpy.abs(cr) >= 1e-3 * numpy.abs(cr).max()
     assert numpy.max(numpy.abs(cg - cr)[sig] / numpy.abs(cr)[sig]) <= 1e-5
+
+
+GRAD48 = __import__('conftest').GOLDEN / 'grad48.npz'
+
+
+@pytest.mark.skipif(not GRAD48.exists(), reason='tests/golden/grad48.npz not generated')
+def test_autograd_gradient_matches_reference_adjoint_at_48(cuda):
+    """The design problem scaled to 48x48x40 (tests/golden/make_golden.py GRAD48): dL/deps
+    from torch.autograd (GPU forward + adjoint solves) against the reference's own gradient,
+    formed from its generic() and generic(adjoint=True) QMR solves, over the whole design
+    region."""
+    import torch
+    from meanas_b200 import workloads
+    from meanas_b200.autograd import fdfd_solve
+    z = numpy.load(GRAD48)
+    p = workloads.adjoint_design(shape=(48, 48, 40), pml=8, wavelength=26.0, design=(16, 16, 6),
+                                 source_x=12, monitor_x=36)
+    dsl = p.extra['design_slices']
+    assert numpy.array_equal(z['eps_design'], p.epsilon.reshape(3, *p.shape)[(slice(None), *dsl)])
+    mon = torch.as_tensor(p.extra['monitor'], device=cuda)
+    eps = torch.as_tensor(p.epsilon, device=cuda).requires_grad_(True)
+    E = fdfd_solve(eps, p.J, p.omega, p.dxes, rtol=1e-12)
+    L = (E.abs() ** 2)[mon].sum()
+    L.backward()
+    g = eps.grad.cpu().numpy().reshape(3, *p.shape)[(slice(None), *dsl)]
+    ref = z['grad_design']
+    tol = max(1e-6, 100 * float(z['rtol']))   # the reference's QMR tolerance bounds its accuracy
+    assert abs(L.item() - float(z['loss'])) <= tol * float(z['loss'])
+    assert numpy.linalg.norm(g - ref) <= tol * numpy.linalg.norm(ref)
